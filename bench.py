@@ -1,0 +1,429 @@
+"""Benchmark of the fused D3Q19 BGK time step on B200.
+
+Workload (one "step" = one time step of the whole lattice): the Taylor-Green
+vortex, 256^3 fully periodic, FP32 storage and compute, tau = 3 nu + 0.5 with
+nu = u0 * 256 / 1600, u0 = 0.05.  The state (2 x 19 arrays, 2.6 GB) is far
+larger than the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  For N > 1 (torchrun) every rank advances its
+own replica (the path has no exchange step: replicas only) and value is the
+sum of all ranks' lattice updates over the max-over-ranks device time.
+`--impl reference` times the CPU restatement of the reference loops
+(oracle/, OpenMP on all host cores) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L_, M_, N_ = 256, 256, 256
+U0 = 0.05
+NU = U0 * L_ / 1600.0
+TAU = 3.0 * NU + 0.5
+OMEGA = 1.0 / TAU
+B_ALG_F32 = 2 * 19 * 4          # algorithmic bytes per lattice update (FP32)
+WORKLOAD = "taylor_green_256^3_f32_periodic"
+METRIC = "GLUPS (D3Q19 BGK fused move+collide + boundaries, 1 lattice update = 1 node x 1 step)"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_from_profile():
+    """dram bytes per sweep launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "sweep_ab_f32_tgv256.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip().split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sms.append(float(parts[0]))
+                maxs.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sms:
+            return None
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxs), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def make_tgv_state(dev_lat):
+    import torch
+    from bgk3d_gpu_b200 import fields as F
+    rho, ux, uy, uz = F.taylor_green_fields(L_, M_, N_, U0, device="cuda")
+    feq = F.equilibrium_shifted_torch(rho, ux, uy, uz, torch.float32)
+    del rho, ux, uy, uz
+    for d in range(19):
+        dev_lat._a[d][1:N_ + 1, 1:M_ + 1, 1:L_ + 1].copy_(feq[d])
+        if d < 18:
+            dev_lat._b[d].copy_(dev_lat._a[d])
+    del feq
+    torch.cuda.synchronize()
+
+
+def cpu_sample(seconds: float = 12.0, kind: int = 1):
+    """Time the oracle (OpenMP, all cores) on the TGV lattice; returns (GLUPS, cores, sample)."""
+    import numpy as np
+    from oracle import oracle as O
+    from bgk3d_gpu_b200 import fields as F
+    nz = 16  # sample: a 256 x 256 x 16 periodic slab of the same flow per step
+    lat = O.OracleLattice(L_, M_, nz, kind)
+    import torch
+    rho, ux, uy, uz = F.taylor_green_fields(L_, M_, nz, U0)
+    feq = F.equilibrium_shifted_torch(rho, ux, uy, uz, torch.float64).numpy()
+    full = np.zeros((19, nz + 2, M_ + 2, L_ + 2))
+    full[:, 1:nz + 1, 1:M_ + 1, 1:L_ + 1] = feq
+    lat.set_state(F.to_storage_bits(full, kind))
+    lat.step(O.BC_PERIODIC, OMEGA, 1)           # warm
+    t0 = time.perf_counter()
+    steps = 0
+    while time.perf_counter() - t0 < seconds:
+        lat.step(O.BC_PERIODIC, OMEGA, 1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    glups = L_ * M_ * nz * steps / dt / 1e9
+    return glups, lat.nthreads, f"{steps} steps of a {L_}x{M_}x{nz} periodic slab of the TGV flow, {dt:.1f} s"
+
+
+def run_reference_arm(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    import numpy as np
+    from oracle import oracle as O
+    from bgk3d_gpu_b200 import fields as F
+    import torch
+    # one calibration step to size the per-step sample so the run takes about a minute
+    nz = 8
+    lat = O.OracleLattice(L_, M_, nz, O.KIND_F32)
+    rho, ux, uy, uz = F.taylor_green_fields(L_, M_, nz, U0)
+    feq = F.equilibrium_shifted_torch(rho, ux, uy, uz, torch.float64).numpy()
+    full = np.zeros((19, nz + 2, M_ + 2, L_ + 2))
+    full[:, 1:nz + 1, 1:M_ + 1, 1:L_ + 1] = feq
+    lat.set_state(F.to_storage_bits(full, O.KIND_F32))
+    t0 = time.perf_counter()
+    lat.step(O.BC_PERIODIC, OMEGA, 1)
+    per_node = (time.perf_counter() - t0) / (L_ * M_ * nz)
+    total = args.steps + args.warmup
+    budget = 60.0
+    nodes_per_step = max(L_ * M_ * 1, min(L_ * M_ * N_, int(budget / max(total, 1) / per_node)))
+    nzs = max(1, min(N_, nodes_per_step // (L_ * M_)))
+    lat = O.OracleLattice(L_, M_, nzs, O.KIND_F32)
+    full = np.zeros((19, nzs + 2, M_ + 2, L_ + 2))
+    rho, ux, uy, uz = F.taylor_green_fields(L_, M_, nzs, U0)
+    full[:, 1:nzs + 1, 1:M_ + 1, 1:L_ + 1] = F.equilibrium_shifted_torch(rho, ux, uy, uz, torch.float64).numpy()
+    lat.set_state(F.to_storage_bits(full, O.KIND_F32))
+    lat.step(O.BC_PERIODIC, OMEGA, args.warmup)
+    t0 = time.perf_counter()
+    lat.step(O.BC_PERIODIC, OMEGA, args.steps)
+    dt = time.perf_counter() - t0
+    glups = L_ * M_ * nzs * args.steps / dt / 1e9
+    sample = (f"each step: one time step of a {L_}x{M_}x{nzs} periodic slab of the {WORKLOAD} flow "
+              f"(CPU restatement of SRC/col_MC.F90 + SRC/bcond.periodic.F90, no Fortran compiler on the box)")
+    line = {
+        "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (Taylor-Green vortex)",
+        "config": {"workload": WORKLOAD, "l": L_, "m": M_, "n": N_, "tau": TAU, "u0": U0},
+        "impl": "reference",
+        "cpu_baseline": {"value": glups, "unit": "GLUPS", "cores": lat.nthreads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": glups, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def ref_cuda_glups(steps: int = 200):
+    """The reference's own native CUDA port (SRC/col_MC_gpu.hpp + SRC/bcond_gpu.hpp,
+    compiled for sm_100a from its sources into oracle/_ref) on the same workload."""
+    import torch
+    path = os.path.join(ROOT, "oracle", "_ref", "libbgkref_sp.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    lib.col_mc_gpu.argtypes = [ctypes.c_void_p] * 37 + [ctypes.c_int] * 5 + [ctypes.c_float] * 12
+    lib.bcond_periodic_gpu.argtypes = [ctypes.POINTER(ctypes.c_void_p)] + [ctypes.c_int] * 5
+    from bgk3d_gpu_b200.lattice import DeviceLattice
+    lat = DeviceLattice(L_, M_, N_, kind="f32", bcase="periodic", omega=OMEGA)
+    make_tgv_state(lat)
+    a, b = list(lat._a), list(lat._b)
+    nx, ny = L_ + 2, M_ + 2
+
+    def step():
+        pa = (ctypes.c_void_p * 19)(*[t.data_ptr() for t in a])
+        lib.bcond_periodic_gpu(pa, L_, M_, N_, nx, ny)
+        lib.col_mc_gpu(*[t.data_ptr() for t in a], *[t.data_ptr() for t in b], L_, M_, N_, nx, ny,
+                       OMEGA, 0.0, 1.0, 1 / 3, 1 / 18, 1 / 36, 3.0, 1.5, 3.0, 0.0, 0.0, 0.0)
+        for d in range(18):
+            a[d], b[d] = b[d], a[d]
+
+    for _ in range(5):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(torch.cuda.default_stream())
+    for _ in range(steps):
+        step()
+    e1.record(torch.cuda.default_stream())
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    del lat
+    torch.cuda.empty_cache()
+    return L_ * M_ * N_ * steps / (ms * 1e-3) / 1e9
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from bgk3d_gpu_b200 import _lib
+    from bgk3d_gpu_b200.lattice import DeviceLattice
+    lat = DeviceLattice(L_, M_, N_, kind="f32", bcase="periodic", omega=OMEGA)
+    make_tgv_state(lat)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        lat.sweep()
+    torch.cuda.synchronize()
+    _barrier(ws)
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    _barrier(ws)
+    e0.record(stream)
+    for _ in range(args.steps):
+        lat.sweep()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = _max_over_ranks(ms, ws)
+    nodes = L_ * M_ * N_
+    value = nodes * args.steps * ws / (ms_max * 1e-3) / 1e9
+    launch_s = ms * 1e-3 / args.steps
+    achieved = B_ALG_F32 * nodes / launch_s / 1e9
+    peak, peak_src = _peaks()
+    ke = lat.moments()
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "GLUPS", "steps": args.steps,
+                              "ms_per_step": ms_max / args.steps, "config": {"l": L_, "m": M_, "n": N_},
+                              "achieved_gbs": achieved, "kernel_only": True}), flush=True)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+    # ---- e2e through the reference-facing drop-in ABI with host buffers --------
+    e2e = run_e2e(lat, args)
+    del lat
+    torch.cuda.empty_cache()
+    ref_cuda = ref_cuda_glups() if rank == 0 else None
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    cpu = cpu_sample()
+    traffic = _traffic_from_profile()
+    line = {
+        "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (Taylor-Green vortex initial condition, BASELINE form)",
+        "config": {"workload": WORKLOAD, "l": L_, "m": M_, "n": N_, "tau": TAU, "u0": U0,
+                   "pattern": "AB two-lattice, boundaries fused",
+                   "l2": "inputs 2.6 GB > 126 MB L2 (no flush needed)",
+                   "parallelism": f"replicas x{ws}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src,
+                     "traffic": traffic, "b_alg_per_lup": B_ALG_F32,
+                     "kernel": "sweep_ab_kernel<float,float,PERIODIC>"},
+        "cpu_baseline": {"value": cpu[0], "unit": "GLUPS", "cores": cpu[1], "kind": "port",
+                         "sample": cpu[2]},
+        "e2e": e2e,
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "ref_cuda_sm100a_glups": ref_cuda,
+        "mass_sum_final": float(ke[0]), "ke_mean_final": float(ke[4] / nodes),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_e2e(lat, args):
+    """Same workload through the reference's C ABI (bcond_periodic_gpu + col_mc_gpu
+    of libbgk3d_dropin_sp.so), from pinned host memory: H2D of the initial
+    state, every step the FP64 kinetic-energy reduction read back to the host,
+    D2H of the final state."""
+    import torch
+    from bgk3d_gpu_b200 import _lib
+    D = _lib.load_dropin(False)
+    L = _lib.lib()
+    host = torch.stack([t for t in lat._a]).cpu().pin_memory()
+    host_out = torch.empty_like(host).pin_memory()
+    ke_host = torch.empty(5, dtype=torch.float64).pin_memory()
+    A = torch.empty_like(lat.A)
+    B = torch.empty_like(lat.B)
+    a = [A[d] for d in range(19)]
+    b = [B[d] for d in range(18)]
+    nx, ny = L_ + 2, M_ + 2
+    ws_bytes = L.bgk_reduce_workspace_bytes(L_, M_, N_)
+    wsp = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    out = torch.empty(5, dtype=torch.float64, device="cuda")
+    p = _lib.sweep_params(_lib.KIND_F32, L_, M_, N_, OMEGA)
+    stream = torch.cuda.default_stream()
+    steps = max(10, args.steps // 4)
+
+    def one_run(nsteps):
+        A.copy_(host, non_blocking=True)
+        for _ in range(nsteps):
+            pa = (ctypes.c_void_p * 19)(*[t.data_ptr() for t in a])
+            D.bcond_periodic_gpu(pa, L_, M_, N_, nx, ny)
+            D.col_mc_gpu(*[t.data_ptr() for t in a], *[t.data_ptr() for t in b], L_, M_, N_, nx, ny,
+                         OMEGA, 0.0, 1.0, 1 / 3, 1 / 18, 1 / 36, 3.0, 1.5, 3.0, 0.0, 0.0, 0.0)
+            for d in range(18):
+                a[d], b[d] = b[d], a[d]
+            _lib.check(L.bgk_moments(ctypes.byref(p), _lib.ptr_array([t.data_ptr() for t in a]),
+                                     out.data_ptr(), wsp.data_ptr(), ws_bytes, None), "bgk_moments")
+            ke_host.copy_(out, non_blocking=True)
+            stream.synchronize()
+        host_out.copy_(torch.stack(a), non_blocking=True)
+        stream.synchronize()
+
+    with torch.cuda.stream(stream):
+        one_run(3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one_run(steps)
+        dt = time.perf_counter() - t0
+    state_bytes = host.numel() * host.element_size()
+    return {"value": L_ * M_ * N_ * steps / dt / 1e9, "unit": "GLUPS",
+            "h2d_bytes_per_step": state_bytes / steps,
+            "d2h_bytes_per_step": state_bytes / steps + 40,
+            "steps": steps,
+            "path": "drop-in C ABI (bcond_periodic_gpu + col_mc_gpu) + per-step FP64 KE to host"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--lattice", type=int, nargs=3, default=None, metavar=("L", "M", "N"),
+                    help="override the lattice extents (profiling runs of a smaller case)")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="time the sweep only (no e2e, CPU or reference-CUDA legs): for ncu captures")
+    args = ap.parse_args()
+    if args.lattice:
+        global L_, M_, N_
+        L_, M_, N_ = args.lattice
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

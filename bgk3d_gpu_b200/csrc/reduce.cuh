@@ -1,0 +1,148 @@
+// FP64 global reductions over a lattice: per-node quantities in the compute
+// type (as the reference computes them), accumulated in double with warp
+// shuffles, a shared-memory block stage and a deterministic second pass over
+// the per-block partials (fixed order, so repeated calls give identical bits).
+#pragma once
+#include "d3q19.cuh"
+
+namespace bgk {
+
+template <class S, class C> struct FieldArgs {
+    const S* a[19];
+    long long nx, nxy;
+    int l, m, n;
+    C cte1;
+    float inv_scale;
+    const int* obs;      // optional: nodes with obs==1 are skipped
+    long long obs_nx, obs_nxy;
+    int imin, imax, jmin, jmax, kmin, kmax;   // obstacle bbox
+};
+
+template <int NQ>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NQ], double* partial) {
+    __shared__ double sm[32][NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
+    const int lane = tid & 31, warp = tid >> 5, nw = (nthr + 31) >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) sm[warp][q] = v[q];
+    __syncthreads();
+    if (tid == 0) {
+        const long long bid = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+        for (int q = 0; q < NQ; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += sm[w][q];
+            partial[bid * NQ + q] = s;
+        }
+    }
+}
+
+template <class S, class C>
+__device__ __forceinline__ bool is_solid(const FieldArgs<S, C>& P, int i, int j, int k) {
+    if (P.obs == nullptr || i < P.imin || i > P.imax || j < P.jmin || j > P.jmax || k < P.kmin ||
+        k > P.kmax)
+        return false;
+    return P.obs[(long long)(i - 1) + P.obs_nx * (j - 1) + P.obs_nxy * (k - 1)] == 1;
+}
+
+// Per-node rho, u and 0.5|u|^2 of the stored (post-collision) state, the
+// arithmetic of SRC/diagno.F90:112-127.  Sums over fluid nodes.
+// grid = (ceil(l/TX), ceil(m/TY), KB); blocks stride over k.
+template <class S, class C>
+__global__ void __launch_bounds__(256) moments_partial_kernel(const FieldArgs<S, C> P, double* partial) {
+    const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    double v[5] = {0, 0, 0, 0, 0};
+    if (i <= P.l && j <= P.m) {
+        for (int k = 1 + (int)blockIdx.z; k <= P.n; k += (int)gridDim.z) {
+            if (is_solid(P, i, j, k)) continue;
+            const long long c = (long long)i + P.nx * (long long)j + P.nxy * (long long)k;
+            C x[19];
+#pragma unroll
+            for (int d = 0; d < 19; ++d) x[d] = Conv<S, C>::ld(P.a[d][c], P.inv_scale);
+            const C rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] +
+                          x[10] + x[11] + x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18] + P.cte1;
+            const C rhoinv = C(1) / rho;
+            const C xj = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * rhoinv;
+            const C yj = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * rhoinv;
+            const C zj = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * rhoinv;
+            v[0] += (double)rho;
+            v[1] += (double)xj;
+            v[2] += (double)yj;
+            v[3] += (double)zj;
+            v[4] += (double)(C(0.5) * (xj * xj + yj * yj + zj * zj));
+        }
+    }
+    block_reduce_store<5>(v, partial);
+}
+
+// Momentum-exchange force on the obstacle, SRC/draglift.F90:77-176:
+// F_a = sum over fluid nodes x in the box of sum_p 2 c_pa a_p(x) obs(x + c_p).
+// grid covers the box; one node per thread.
+template <class S, class C>
+__global__ void __launch_bounds__(256) draglift_partial_kernel(const FieldArgs<S, C> P, int is, int js,
+                                                               int ks, int ni, int nj, int nk,
+                                                               double* partial) {
+    double v[3] = {0, 0, 0};
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long tot = (long long)ni * nj * nk;
+    if (t < tot) {
+        const int i = is + (int)(t % ni);
+        const int j = js + (int)((t / ni) % nj);
+        const int k = ks + (int)(t / ((long long)ni * nj));
+        if (i >= 1 && i <= P.l && j >= 1 && j <= P.m && k >= 1 && k <= P.n && !is_solid(P, i, j, k)) {
+            const long long c = (long long)i + P.nx * (long long)j + P.nxy * (long long)k;
+            C ap[18];
+            C ob[18];
+#pragma unroll
+            for (int d = 0; d < 18; ++d) {
+                ap[d] = Conv<S, C>::ld(P.a[d][c], P.inv_scale);
+                ob[d] = is_solid(P, i + cx_of(d), j + cy_of(d), k + cz_of(d)) ? C(1) : C(0);
+            }
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+                C s = C(0);
+#pragma unroll
+                for (int d = 0; d < 18; ++d) {
+                    const int cc = ax == 0 ? cx_of(d) : (ax == 1 ? cy_of(d) : cz_of(d));
+                    const C term = C(2.0) * (C)cc * ap[d] * ob[d];
+                    s = (d == 0) ? term : s + term;
+                }
+                v[ax] = (double)s;
+            }
+        }
+    }
+    block_reduce_store<3>(v, partial);
+}
+
+// Second pass: one block sums nparts partials of NQ values in a fixed order.
+template <int NQ>
+__global__ void __launch_bounds__(256) finalize_partials_kernel(const double* partial, long long nparts,
+                                                                double* out) {
+    __shared__ double sm[256][NQ];
+    double v[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] = 0.0;
+    for (long long p = threadIdx.x; p < nparts; p += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) v[q] += partial[p * NQ + q];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sm[threadIdx.x][q] = v[q];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) sm[threadIdx.x][q] += sm[threadIdx.x + s][q];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) out[q] = sm[0][q];
+}
+
+}  // namespace bgk

@@ -1,0 +1,217 @@
+// Fused boundary + pull-stream + BGK collide sweep, two-lattice (A -> B)
+// pattern, on the reference's structure-of-arrays layout.
+//
+// What one launch computes is what the reference computes with
+//   bcond_<case> (SRC/bcond.<case>.F90, x -> y -> z halo writes)
+//   bcond_obs    (SRC/bcond.obs.F90:103-122, writes into solid nodes)
+//   col_MC       (SRC/col_MC.F90:255-536, pull from a, write b / a19)
+// for every fluid node, without materialising the halo: each link whose
+// source x - c_p lies outside the lattice (or in a solid node) is resolved in
+// registers by the rule the reference's halo writes produce:
+//   * a wall face (driven: all six, channel: z) -> the node's own opposite
+//     population (half-way bounce-back), plus the lid term on pops 02/11 at
+//     the top face (SRC/bcond.driven.F90:243-246; the z loop runs last, so it
+//     wins at every edge);
+//   * periodic axes -> the wrapped node (the full-range x, y, z copies of
+//     SRC/bcond.periodic.F90 make every edge and corner a double/triple wrap);
+//   * inflow face x=0 -> the equilibrium at rho=1, u=(u_in,0,0)
+//     (SRC/bcond.inflow.F90:165-181), rounded to storage precision;
+//   * outflow face x=l+1 -> the halo plane written by outflow_halo_kernel
+//     (SRC/bcond.inflow.F90:135-162), read at the y/z-wrapped position;
+//   * a solid neighbour (obs==1) -> own opposite population.
+// Values that the reference constructs arithmetically before storing them in
+// the halo (lid, inflow) are rounded through the storage type, so 16-bit and
+// mixed kinds see exactly the reference's stored value.
+//
+// Solid nodes are not updated (their reference values are racy garbage: see
+// SRC/bcond_gpu.hpp:438-455).  An obstacle must keep one node away from the
+// faces (validated by the host), because the reference's periodic and outflow
+// copies would otherwise read solid-node garbage.
+#pragma once
+#include "d3q19.cuh"
+
+namespace bgk {
+
+template <class S, class C> struct SweepArgs {
+    const S* a[19];   // current populations (a[18] is also written: in place)
+    S* b[19];         // next populations; b[18] is ignored (pop 19 stays in a)
+    long long nx, nxy;
+    int l, m, n;
+    ColConst<C> col;
+    C lid_force;      // driven: added to pop 02 / subtracted from pop 11 at z = n+1
+    C u_inflow;       // inflow: prescribed x velocity at x = 0
+    C inflow_cte1;    // inflow equilibrium constant (0 for shifted storage)
+    float scale, inv_scale;
+    const int* obs;   // optional: obstacle mask, Fortran layout (1:l,1:m,1:n)
+    long long obs_nx, obs_nxy;
+    int imin, imax, jmin, jmax, kmin, kmax;
+};
+
+// Equilibrium population p (0..4 -> 01..05) of the inflow face
+// (SRC/bcond.inflow.F90:165-181), in the compute type.
+template <class C>
+__device__ __forceinline__ C inflow_eq(int p, C u_in, C cte1, const ColConst<C>& K) {
+    const C rf = K.rf, qf = K.qf, three = C(3), crho = C(1);
+    const C xj = u_in, yj = C(0), zj = C(0);
+    const C cvsq = xj * xj + yj * yj + zj * zj;
+    C cxp;
+    switch (p) {
+        case 0: cxp = rf * (xj - yj) + qf * (three * (xj - yj) * (xj - yj) - cvsq); break;
+        case 1: cxp = rf * (xj - zj) + qf * (three * (xj - zj) * (xj - zj) - cvsq); break;
+        case 2: cxp = rf * (xj + yj) + qf * (three * (xj + yj) * (xj + yj) - cvsq); break;
+        case 3: cxp = rf * (xj + zj) + qf * (three * (xj + zj) * (xj + zj) - cvsq); break;
+        default: cxp = rf * (xj) + qf * (three * (xj) * (xj) - cvsq); break;
+    }
+    const C w = (p == 4) ? K.p1 : K.p2;
+    return crho * w * (cte1 + cxp);
+}
+
+template <class S, class C>
+__device__ __forceinline__ C roundtrip(C v, float scl, float inv) {
+    return Conv<S, C>::ld(Conv<S, C>::st(v, scl), inv);
+}
+
+// Pull of population D at node (i,j,k) through the boundary rules above.
+template <class S, class C, int BC, int D>
+__device__ __forceinline__ C pull_general(const SweepArgs<S, C>& P, int i, int j, int k,
+                                          long long c, uint32_t solid_links) {
+    constexpr int cx = cx_of(D), cy = cy_of(D), cz = cz_of(D), od = opp_of(D);
+    int si = i - cx, sj = j - cy, sk = k - cz;
+    const bool ox = (cx == 1 && i == 1) || (cx == -1 && i == P.l);
+    const bool oy = (cy == 1 && j == 1) || (cy == -1 && j == P.m);
+    const bool oz = (cz == 1 && k == 1) || (cz == -1 && k == P.n);
+    const float inv = P.inv_scale;
+    if (BC == BC_DRIVEN) {
+        if (ox || oy || oz) {
+            C v = Conv<S, C>::ld(P.a[od][c], inv);
+            if (D == 1 && sk == P.n + 1) v = roundtrip<S, C>(v + P.lid_force, P.scale, inv);
+            if (D == 10 && sk == P.n + 1) v = roundtrip<S, C>(v - P.lid_force, P.scale, inv);
+            return v;
+        }
+    } else if (BC == BC_CHANNEL) {
+        if (oz) return Conv<S, C>::ld(P.a[od][c], inv);
+        if (ox) si = (cx == 1) ? P.l : 1;
+        if (oy) sj = (cy == 1) ? P.m : 1;
+    } else if (BC == BC_PERIODIC) {
+        if (ox) si = (cx == 1) ? P.l : 1;
+        if (oy) sj = (cy == 1) ? P.m : 1;
+        if (oz) sk = (cz == 1) ? P.n : 1;
+    } else if (BC == BC_INFLOW) {
+        if (cx == 1 && ox) {
+            if (D < 5) return roundtrip<S, C>(inflow_eq<C>(D, P.u_inflow, P.inflow_cte1, P.col), P.scale, inv);
+        }
+        if (oy) sj = (cy == 1) ? P.m : 1;
+        if (oz) sk = (cz == 1) ? P.n : 1;
+    }
+    if (!(ox || oy || oz) && ((solid_links >> D) & 1u)) return Conv<S, C>::ld(P.a[od][c], inv);
+    const long long s = (long long)si + P.nx * (long long)sj + P.nxy * (long long)sk;
+    if (D == 18) return Conv<S, C>::ld(P.a[18][s], inv);
+    return Conv<S, C>::ld(ldro<S>(P.a[D] + s), inv);
+}
+
+template <class S, class C, int BC, int D>
+struct PullAll {
+    __device__ __forceinline__ static void run(const SweepArgs<S, C>& P, int i, int j, int k,
+                                               long long c, uint32_t sl, C (&x)[19]) {
+        x[D] = pull_general<S, C, BC, D>(P, i, j, k, c, sl);
+        PullAll<S, C, BC, D + 1>::run(P, i, j, k, c, sl, x);
+    }
+};
+template <class S, class C, int BC>
+struct PullAll<S, C, BC, 19> {
+    __device__ __forceinline__ static void run(const SweepArgs<S, C>&, int, int, int, long long,
+                                               uint32_t, C (&)[19]) {}
+};
+
+// Bit D set when the source x - c_D of node (i,j,k) is a solid node; bit 31
+// when the node itself is solid.
+template <class S, class C>
+__device__ __forceinline__ uint32_t obstacle_links(const SweepArgs<S, C>& P, int i, int j, int k) {
+    uint32_t bits = 0;
+    auto solid = [&](int si, int sj, int sk) -> bool {
+        if (si < P.imin || si > P.imax || sj < P.jmin || sj > P.jmax || sk < P.kmin || sk > P.kmax)
+            return false;
+        const long long o = (long long)(si - 1) + P.obs_nx * (long long)(sj - 1) +
+                            P.obs_nxy * (long long)(sk - 1);
+        return __ldg(P.obs + o) == 1;
+    };
+    if (solid(i, j, k)) return 0x80000000u;
+#pragma unroll
+    for (int d = 0; d < 18; ++d)
+        if (solid(i - cx_of(d), j - cy_of(d), k - cz_of(d))) bits |= 1u << d;
+    return bits;
+}
+
+// One thread per interior node; blockDim = (TX, TY), grid = (ceil(l/TX), ceil(m/TY), n).
+template <class S, class C, int BC>
+__global__ void __launch_bounds__(256) sweep_ab_kernel(const SweepArgs<S, C> P) {
+    const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    const int k = 1 + (int)blockIdx.z;
+    if (i > P.l || j > P.m) return;
+    const long long c = (long long)i + P.nx * (long long)j + P.nxy * (long long)k;
+
+    uint32_t sl = 0;
+    if (P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
+        j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1) {
+        sl = obstacle_links(P, i, j, k);
+        if (sl & 0x80000000u) return;   // solid node: not updated
+    }
+    const bool edge = (BC != BC_NONE) &&
+                      (i == 1 || i == P.l || j == 1 || j == P.m || k == 1 || k == P.n);
+    const float inv = P.inv_scale;
+    C x[19];
+    if (!edge && sl == 0) {
+        const long long nx = P.nx, nxy = P.nxy;
+#pragma unroll
+        for (int d = 0; d < 18; ++d) {
+            const long long s = c - cx_of(d) - cy_of(d) * nx - cz_of(d) * nxy;
+            x[d] = Conv<S, C>::ld(ldro<S>(P.a[d] + s), inv);
+        }
+        x[18] = Conv<S, C>::ld(P.a[18][c], inv);
+    } else {
+        PullAll<S, C, BC, 0>::run(P, i, j, k, c, sl, x);
+    }
+    C y[19];
+    bgk_collide<C>(x, y, P.col);
+    const float scl = P.scale;
+#pragma unroll
+    for (int d = 0; d < 18; ++d) P.b[d][c] = Conv<S, C>::st(y[d], scl);
+    const_cast<S*>(P.a[18])[c] = Conv<S, C>::st(y[18], scl);
+}
+
+// Outflow halo plane for the inflow case: a10..a14(l+1, j, k) from the
+// moments of node (l, j, k) at rho = 1 (SRC/bcond.inflow.F90:135-162), over
+// j = 1..m, k = 1..n (the sweep reads the y/z-wrapped position, which is
+// always one of these).
+template <class S, class C>
+__global__ void outflow_halo_kernel(const SweepArgs<S, C> P) {
+    const int j = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int k = 1 + (int)blockIdx.y;
+    if (j > P.m) return;
+    const float inv = P.inv_scale, scl = P.scale;
+    const long long c = (long long)P.l + P.nx * (long long)j + P.nxy * (long long)k;
+    C a[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) a[d] = Conv<S, C>::ld(P.a[d][c], inv);
+    const C rhoinv = C(1), crho = C(1), rf = P.col.rf, qf = P.col.qf, three = C(3);
+    const C cte1 = P.inflow_cte1, p1 = P.col.p1, p2 = P.col.p2;
+    const C xj = (a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13]) * rhoinv;
+    const C yj = (a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17]) * rhoinv;
+    const C zj = (a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15]) * rhoinv;
+    const C cvsq = xj * xj + yj * yj + zj * zj;
+    const C cx10 = rf * (-xj - yj) + qf * (three * (xj + yj) * (xj + yj) - cvsq);
+    const C cx11 = rf * (-xj - zj) + qf * (three * (xj + zj) * (xj + zj) - cvsq);
+    const C cx12 = rf * (-xj + yj) + qf * (three * (xj - yj) * (xj - yj) - cvsq);
+    const C cx13 = rf * (-xj + zj) + qf * (three * (xj - zj) * (xj - zj) - cvsq);
+    const C cx14 = rf * (-xj) + qf * (three * (xj) * (xj) - cvsq);
+    const long long h = c + 1;
+    S** A = const_cast<S**>(P.a);
+    A[9][h] = Conv<S, C>::st(crho * p2 * (cte1 + cx10), scl);
+    A[10][h] = Conv<S, C>::st(crho * p2 * (cte1 + cx11), scl);
+    A[11][h] = Conv<S, C>::st(crho * p2 * (cte1 + cx12), scl);
+    A[12][h] = Conv<S, C>::st(crho * p2 * (cte1 + cx13), scl);
+    A[13][h] = Conv<S, C>::st(crho * p1 * (cte1 + cx14), scl);
+}
+
+}  // namespace bgk

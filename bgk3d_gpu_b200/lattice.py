@@ -1,0 +1,131 @@
+"""Python host side of the library: a reference-layout lattice on the device
+(memory from torch), advanced through the C ABI of libbgk3d_b200.so.
+
+`DeviceLattice` mirrors the reference's driver loop for one case
+(SRC/bgk3d.F90:169-179: boundaries -> col_MC -> pointer swap) with the
+boundary fused into the sweep, and its diagnostics (SRC/diagno.F90,
+SRC/draglift.F90) as FP64 device reductions.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import BC_NAMES, KIND_NAMES, check, lib, ptr_array, sweep_params
+
+TORCH_DTYPE = {0: torch.float64, 1: torch.float32, 2: torch.float16, 3: torch.bfloat16,
+               4: torch.float32}
+
+
+def _kind(k) -> int:
+    return KIND_NAMES[k] if isinstance(k, str) else int(k)
+
+
+def _bcase(b) -> int:
+    return BC_NAMES[b] if isinstance(b, str) else int(b)
+
+
+class DeviceLattice:
+    """19 'a' + 18 'b' device arrays in the reference layout, pop 19 in place."""
+
+    def __init__(self, l, m, n, kind="f32", bcase="periodic", omega=1.0, ipad=0, jpad=0,
+                 device="cuda", scale=1.0, lid_force=0.0, u_inflow=0.0, inflow_cte1=0.0,
+                 force_mode=0, force=(0.0, 0.0, 0.0), cte1=1.0):
+        self.l, self.m, self.n = l, m, n
+        self.kind, self.bcase = _kind(kind), _bcase(bcase)
+        self.nx, self.ny, self.nz = l + 2 + ipad, m + 2 + jpad, n + 2
+        self.device = torch.device(device)
+        dt = TORCH_DTYPE[self.kind]
+        self.A = torch.zeros((19, self.nz, self.ny, self.nx), dtype=dt, device=self.device)
+        self.B = torch.zeros((18, self.nz, self.ny, self.nx), dtype=dt, device=self.device)
+        self._a = [self.A[d] for d in range(19)]
+        self._b = [self.B[d] for d in range(18)]
+        self.obs = None
+        self.params = sweep_params(self.kind, l, m, n, omega, bcase=self.bcase, nx=self.nx,
+                                   ny=self.ny, scale=scale, lid_force=lid_force, u_inflow=u_inflow,
+                                   inflow_cte1=inflow_cte1, force_mode=force_mode,
+                                   fx=force[0], fy=force[1], fz=force[2], cte1=cte1,
+                                   cte0=1.0 - cte1)
+        self._ws = None
+        self._out = torch.zeros(8, dtype=torch.float64, device=self.device)
+        self.steps_done = 0
+
+    # ------------------------------------------------------------ state I/O
+    def upload(self, state: np.ndarray) -> None:
+        """state: (19, nz, ny, nx) in the storage representation (uint16 bits for 16-bit kinds)."""
+        t = torch.from_numpy(np.ascontiguousarray(state))
+        if self.kind in (2, 3):
+            t = t.view(torch.int16).view(TORCH_DTYPE[self.kind])
+        for d in range(19):
+            self._a[d].copy_(t[d].to(self.device))
+        for d in range(18):
+            self._b[d].copy_(t[d].to(self.device))
+
+    def download(self) -> np.ndarray:
+        """Current (post-collision) state, (19, nz, ny, nx), storage representation."""
+        st = torch.stack([p for p in self._a]).cpu()
+        if self.kind in (2, 3):
+            return st.view(torch.int16).numpy().view(np.uint16)
+        return st.numpy()
+
+    def set_obstacle(self, obs: np.ndarray) -> None:
+        """obs: int32 (n, m, l) [k, j, i], 1 = solid (SRC/build.obs.F90 convention)."""
+        obs = np.ascontiguousarray(obs, np.int32)
+        self.obs = torch.from_numpy(obs).to(self.device)
+        ks, js, is_ = np.nonzero(obs == 1)
+        p = self.params
+        p.obs = self.obs.data_ptr()
+        p.obs_nx, p.obs_ny = self.l, self.m
+        if len(is_):
+            p.imin, p.imax = int(is_.min()) + 1, int(is_.max()) + 1
+            p.jmin, p.jmax = int(js.min()) + 1, int(js.max()) + 1
+            p.kmin, p.kmax = int(ks.min()) + 1, int(ks.max()) + 1
+        else:
+            p.imin, p.imax, p.jmin, p.jmax, p.kmin, p.kmax = 1, 0, 1, 0, 1, 0
+
+    # ------------------------------------------------------------ time loop
+    def _ptrs(self):
+        return (ptr_array([t.data_ptr() for t in self._a]),
+                ptr_array([t.data_ptr() for t in self._b] + [self._a[18].data_ptr()]))
+
+    def sweep(self, stream=None) -> None:
+        """One fused time step (boundaries + stream + collide) and the a<->b swap."""
+        a, b = self._ptrs()
+        st = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
+        check(lib().bgk_sweep(ctypes.byref(self.params), a, b, st), "bgk_sweep")
+        for d in range(18):
+            self._a[d], self._b[d] = self._b[d], self._a[d]
+        self.steps_done += 1
+
+    def step(self, nsteps=1) -> None:
+        for _ in range(nsteps):
+            self.sweep()
+
+    # ---------------------------------------------------------- diagnostics
+    def _workspace(self):
+        if self._ws is None:
+            nb = lib().bgk_reduce_workspace_bytes(self.l, self.m, self.n)
+            self._ws = torch.empty(max(nb, 1 << 16), dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def moments(self) -> np.ndarray:
+        """FP64 sums over fluid nodes: rho, u_x, u_y, u_z, 0.5|u|^2 (SRC/diagno.F90)."""
+        ws = self._workspace()
+        a, _ = self._ptrs()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        check(lib().bgk_moments(ctypes.byref(self.params), a, self._out.data_ptr(), ws.data_ptr(),
+                                ws.numel(), st), "bgk_moments")
+        return self._out[:5].cpu().numpy().copy()
+
+    def draglift(self, box) -> np.ndarray:
+        """FP64 momentum-exchange force (Fx, Fy, Fz) over the box (is, ie, js, je, ks, ke)."""
+        ws = self._workspace()
+        a, _ = self._ptrs()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        check(lib().bgk_draglift(ctypes.byref(self.params), a, *[int(v) for v in box],
+                                 self._out.data_ptr(), ws.data_ptr(), ws.numel(), st),
+              "bgk_draglift")
+        return self._out[:3].cpu().numpy().copy()

@@ -1,0 +1,114 @@
+/*
+ * bgk3d_b200.h -- C ABI of the B200 D3Q19 BGK time-step library
+ * (libbgk3d_b200.so).  Plain pointers and sizes only; all array arguments are
+ * DEVICE pointers unless a parameter name ends in _host.
+ *
+ * Layout contract (the reference's, SRC/alloca.F90:153-191): every population
+ * p = 01..19 is its own array (0:l+1+ipad, 0:m+1+jpad, 0:n+1) with i fastest;
+ * element (i,j,k) is at i + nx*j + nx*ny*k, nx = l+2+ipad, ny = m+2+jpad.
+ * Populations are stored shifted by their weight (f_p - w_p) when cte1 = 1.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   bgk_sweep      <- col_mc_gpu        SRC/col_MC_cuda.cu:16-53 together with
+ *                     bcond_*_gpu       SRC/bcond_gpu.hpp:499-544 (boundaries
+ *                                       fused into the same launch)
+ *   bgk_moments    <- diagno            SRC/diagno.F90:87-138 (host/OpenACC
+ *                                       reduction in the reference)
+ *   bgk_draglift   <- draglift          SRC/draglift.F90:77-181
+ *   bgk_device_sync<- gpu_device_sync   SRC/bcond_gpu.hpp:548-571
+ * The reference-named drop-in symbols themselves are declared in
+ * bgk3d_dropin.h.
+ *
+ * Every function returns BGK_OK (0) or a negative status; bgk_last_error()
+ * returns a message for the calling thread's last failure.
+ */
+#ifndef BGK3D_B200_H
+#define BGK3D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#include <stddef.h>
+#include <stdint.h>
+
+#define BGK_OK 0
+#define BGK_ERR_ARG (-1)
+#define BGK_ERR_CUDA (-2)
+#define BGK_ERR_UNSUPPORTED (-3)
+#define BGK_ERR_NOMEM (-4)
+#define BGK_ERR_STATE (-5)
+
+/* storage / compute precision (SRC/precision.F90:14-47) */
+#define BGK_KIND_F64 0     /* DOUBLE: f64 storage, f64 collision               */
+#define BGK_KIND_F32 1     /* SINGLE: f32 storage, f32 collision               */
+#define BGK_KIND_F16 2     /* f - w stored as binary16 (x scale), f32 collision */
+#define BGK_KIND_BF16 3    /* f - w stored as bfloat16 (x scale), f32 collision */
+#define BGK_KIND_F32_F64 4 /* MIXED2: f32 storage, f64 collision               */
+
+/* boundary case (SRC/boundaries.F90:31-43) */
+#define BGK_BC_NONE (-1)   /* halos are left as the caller prepared them */
+#define BGK_BC_DRIVEN 0    /* six bounce-back walls, moving lid at z = n+1 */
+#define BGK_BC_PERIODIC 1
+#define BGK_BC_CHANNEL 2   /* x, y periodic; z no-slip walls */
+#define BGK_BC_INFLOW 3    /* x: inflow at 0 / outflow at l+1; y, z periodic */
+
+typedef struct bgk_sweep_params {
+    int kind;                 /* BGK_KIND_* */
+    int bcase;                /* BGK_BC_* */
+    int l, m, n;              /* interior extents */
+    long long nx, ny;         /* leading dimensions of each population array */
+    /* collision constants, SRC/col_MC_gpu.hpp:86-94 (bgk_sweep_params_init
+       fills the reference's values) */
+    double omega, cte0, cte1, p0, p1, p2, rf, qf, tre;
+    int force_mode;           /* 0: constant forces (native ABI); 1: force*rho (CHANNEL) */
+    double fx, fy, fz;
+    double lid_force;         /* DRIVEN: u00/6 (SRC/bcond.driven.F90:61) */
+    double u_inflow;          /* INFLOW: prescribed u_x at x = 0 */
+    double inflow_cte1;       /* INFLOW equilibrium constant: 0 for shifted storage */
+    float scale;              /* 16-bit kinds: power-of-two storage scale */
+    const int32_t* obs;       /* optional obstacle mask (1:l,1:m,1:n), obs==1 solid */
+    int obs_nx, obs_ny;       /* its leading dimensions (normally l, m) */
+    int imin, imax, jmin, jmax, kmin, kmax;  /* bounding box of the solid nodes */
+} bgk_sweep_params;
+
+/* Fill *p with the reference's constants (p0 = 1/3, p1 = 1/18, p2 = 1/36,
+   rf = tre = 3, qf = 1.5, cte1 = 1, cte0 = 0), no force, no obstacle,
+   bcase NONE, scale 1, nx = l+2, ny = m+2. */
+void bgk_sweep_params_init(bgk_sweep_params* p, int kind, int l, int m, int n, double omega);
+
+/* One fused time step: boundary rules + pull-stream + BGK collision from the
+   19 arrays a[] into b[0..17] and (in place) a[18].  b[18] is ignored.
+   Stream-ordered, no synchronisation.  For BGK_BC_INFLOW it also writes the
+   outflow halo plane a[9..13](l+1, 1..m, 1..n). */
+int bgk_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, void* stream);
+
+/* Bytes of device workspace bgk_moments / bgk_draglift need for a lattice of
+   these extents (per-block FP64 partial sums). */
+size_t bgk_reduce_workspace_bytes(int l, int m, int n);
+
+/* FP64 sums over fluid nodes of rho, u_x, u_y, u_z, 0.5|u|^2 (per-node values
+   computed as SRC/diagno.F90:112-127) into out_dev[0..4] (device memory).
+   Uses p->kind, l, m, n, nx, ny, cte1, scale, obs/bbox.  Deterministic. */
+int bgk_moments(const bgk_sweep_params* p, void* const* a, double* out_dev, void* workspace,
+                size_t workspace_bytes, void* stream);
+
+/* FP64 momentum-exchange force (Fx, Fy, Fz, unnormalised) on the obstacle,
+   summed over fluid nodes in the box [is..ie]x[js..je]x[ks..ke]
+   (SRC/draglift.F90:77-176) into out_dev[0..2]. */
+int bgk_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
+                 int ke, double* out_dev, void* workspace, size_t workspace_bytes, void* stream);
+
+/* cudaDeviceSynchronize; returns BGK_ERR_CUDA (does not abort) on failure. */
+int bgk_device_sync(void);
+
+/* Message describing the calling thread's last error ("" if none). */
+const char* bgk_last_error(void);
+
+/* Library version string. */
+const char* bgk_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BGK3D_B200_H */
