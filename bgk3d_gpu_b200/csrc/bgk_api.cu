@@ -2,6 +2,7 @@
 // shapes around the kernels of sweep_ab.cuh and reduce.cuh.
 #include <cuda_runtime.h>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <string>
 #include "bgk3d_b200.h"
@@ -97,22 +98,57 @@ SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* cons
     return A;
 }
 
+// Warp-segment launch geometry of sweep_ab_kernel (see sweep_ab.cuh).
+template <class S, class C>
+void segment_geometry(SweepArgs<S, C>& A, const void* a0) {
+    const long long elem = (long long)((uintptr_t)a0 / sizeof(S));
+    A.align_base = elem & 31;
+    const bool aligned = ((A.align_base + 1) % 32 == 0) && (A.nx % 32 == 0);
+    A.nseg_aligned = aligned ? 1 : 0;
+    A.nseg = aligned ? (A.l + 31) / 32 : (A.l + 62) / 32;
+    A.nrows = (uint32_t)((long long)A.m * A.n);
+    A.div_seg.init((uint32_t)A.nseg);
+    A.div_m.init((uint32_t)A.m);
+}
+
+// True unless the collision can use the shifted, force-free specialisation.
+bool generic_collision(const bgk_sweep_params* p) {
+    return !(p->cte1 == 1.0 && p->cte0 == 0.0 && p->fx == 0.0 && p->fy == 0.0 && p->fz == 0.0);
+}
+
+template <class S, class C, int BC>
+void launch_sweep_bc(const SweepArgs<S, C>& A, long long nelem, unsigned blocks, bool generic,
+                     cudaStream_t st) {
+    if (nelem < (1LL << 31)) {
+        if (generic) sweep_ab_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
+        else sweep_ab_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
+    } else {
+        if (generic) sweep_ab_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
+        else sweep_ab_kernel<S, C, BC, long long, false><<<blocks, 256, 0, st>>>(A);
+    }
+}
+
 template <class S, class C>
 int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, cudaStream_t st) {
     SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
+    segment_geometry(A, a[0]);
     if (p->bcase == BC_INFLOW) {
         dim3 blk(128), grd((p->m + 127) / 128, p->n);
         outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
         if (int e = check_launch("outflow_halo_kernel")) return e;
     }
-    dim3 blk = row_block(p->l);
-    dim3 grd((p->l + blk.x - 1) / blk.x, (p->m + blk.y - 1) / blk.y, p->n);
+    const long long warps = (long long)A.nseg * p->m * p->n;
+    const long long blocks = (warps + 7) / 8;
+    if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
+    const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
+    const bool g = generic_collision(p);
+    const unsigned nb = (unsigned)blocks;
     switch (p->bcase) {
-        case BC_NONE: sweep_ab_kernel<S, C, BC_NONE><<<grd, blk, 0, st>>>(A); break;
-        case BC_DRIVEN: sweep_ab_kernel<S, C, BC_DRIVEN><<<grd, blk, 0, st>>>(A); break;
-        case BC_PERIODIC: sweep_ab_kernel<S, C, BC_PERIODIC><<<grd, blk, 0, st>>>(A); break;
-        case BC_CHANNEL: sweep_ab_kernel<S, C, BC_CHANNEL><<<grd, blk, 0, st>>>(A); break;
-        case BC_INFLOW: sweep_ab_kernel<S, C, BC_INFLOW><<<grd, blk, 0, st>>>(A); break;
+        case BC_NONE: launch_sweep_bc<S, C, BC_NONE>(A, nelem, nb, g, st); break;
+        case BC_DRIVEN: launch_sweep_bc<S, C, BC_DRIVEN>(A, nelem, nb, g, st); break;
+        case BC_PERIODIC: launch_sweep_bc<S, C, BC_PERIODIC>(A, nelem, nb, g, st); break;
+        case BC_CHANNEL: launch_sweep_bc<S, C, BC_CHANNEL>(A, nelem, nb, g, st); break;
+        case BC_INFLOW: launch_sweep_bc<S, C, BC_INFLOW>(A, nelem, nb, g, st); break;
     }
     return check_launch("sweep_ab_kernel");
 }

@@ -76,6 +76,26 @@ template <> __device__ __forceinline__ __nv_bfloat16 ldro<__nv_bfloat16>(const _
     return __ushort_as_bfloat16(u);
 }
 
+// Unsigned 32-bit division by a runtime constant with a multiply-high and a
+// shift (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, round-up variant).  Exact for every n < 2^32.
+struct FastDiv {
+    uint32_t d, mul, shift;
+    __host__ void init(uint32_t divisor) {
+        d = divisor;
+        uint32_t l = 0;
+        while ((1ull << l) < divisor) ++l;
+        // mul = floor(2^32 (2^l - d) / d) + 1
+        mul = (uint32_t)((((1ull << l) - divisor) << 32) / divisor + 1);
+        shift = l;
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t n) const {
+        if (shift == 0) return n;   // d == 1
+        const uint32_t t = __umulhi(n, mul);
+        return (t + ((n - t) >> 1)) >> (shift - 1);
+    }
+};
+
 // Collision constants in the compute type.  Weights are computed in double
 // and rounded once, as the reference's parameters are (SRC/storage.F90:58-82,
 // 147-151).
@@ -89,7 +109,12 @@ template <class C> struct ColConst {
 // order of SRC/col_MC.F90:295-379 and :501-519.  The library is compiled with
 // --fmad=false, so every + and * below rounds separately, as in the reference
 // source.  Returns rho, vx, vy, vz (before the rf scaling) through mom[].
-template <class C>
+//
+// GENERIC = false is the specialisation for shifted storage (cte1 = 1,
+// cte0 = 0) without forcing: it omits the terms that are then additions of
+// +0 or multiplications by 1, which changes no result except possibly the
+// sign of an exact zero.
+template <class C, bool GENERIC = true>
 __device__ __forceinline__ void bgk_collide(const C (&x)[19], C (&y)[19], const ColConst<C>& P,
                                             C* mom = nullptr) {
     const C cte0 = P.cte0, cte1 = P.cte1, tre = P.tre, qf = P.qf, rf = P.rf;
@@ -102,28 +127,31 @@ __device__ __forceinline__ void bgk_collide(const C (&x)[19], C (&y)[19], const 
     if (mom) { mom[0] = rho; mom[1] = vx; mom[2] = vy; mom[3] = vz; }
     const C vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
     const C vsq = vx2 + vy2 + vz2;
+    auto q = [&](C t) -> C { return GENERIC ? cte0 + qf * t : qf * t; };
     C vxpy = vx + vy;
-    const C qxpy = cte0 + qf * (tre * vxpy * vxpy - vsq);
+    const C qxpy = q(tre * vxpy * vxpy - vsq);
     C vxmy = vx - vy;
-    const C qxmy = cte0 + qf * (tre * vxmy * vxmy - vsq);
+    const C qxmy = q(tre * vxmy * vxmy - vsq);
     C vxpz = vx + vz;
-    const C qxpz = cte0 + qf * (tre * vxpz * vxpz - vsq);
+    const C qxpz = q(tre * vxpz * vxpz - vsq);
     C vxmz = vx - vz;
-    const C qxmz = cte0 + qf * (tre * vxmz * vxmz - vsq);
+    const C qxmz = q(tre * vxmz * vxmz - vsq);
     C vypz = vy + vz;
-    const C qypz = cte0 + qf * (tre * vypz * vypz - vsq);
+    const C qypz = q(tre * vypz * vypz - vsq);
     C vymz = vy - vz;
-    const C qymz = cte0 + qf * (tre * vymz * vymz - vsq);
-    const C qx = cte0 + qf * (tre * vx2 - vsq);
-    const C qy = cte0 + qf * (tre * vy2 - vsq);
-    const C qz = cte0 + qf * (tre * vz2 - vsq);
-    const C q0 = cte0 + qf * (-vsq);
+    const C qymz = q(tre * vymz * vymz - vsq);
+    const C qx = q(tre * vx2 - vsq);
+    const C qy = q(tre * vy2 - vsq);
+    const C qz = q(tre * vz2 - vsq);
+    const C q0 = q(-vsq);
     vx = rf * vx; vy = rf * vy; vz = rf * vz;
     vxpy = rf * vxpy; vxmy = rf * vxmy; vxpz = rf * vxpz;
     vxmz = rf * vxmz; vypz = rf * vypz; vymz = rf * vymz;
     const C p0 = P.p0, p1 = P.p1, p2 = P.p2;
     const C rp0 = rho * p0, rp1 = rho * p1, rp2 = rho * p2;
-    const C s2 = cte1 * (rp2 - p2), s1 = cte1 * (rp1 - p1), s0 = cte1 * (rp0 - p0);
+    const C s2 = GENERIC ? cte1 * (rp2 - p2) : rp2 - p2;
+    const C s1 = GENERIC ? cte1 * (rp1 - p1) : rp1 - p1;
+    const C s0 = GENERIC ? cte1 * (rp0 - p0) : rp0 - p0;
     C e[19];
     e[0] = rp2 * (+vxmy + qxmy) + s2;
     e[1] = rp2 * (+vxmz + qxmz) + s2;
@@ -144,9 +172,13 @@ __device__ __forceinline__ void bgk_collide(const C (&x)[19], C (&y)[19], const 
     e[16] = rp1 * (-vy + qy) + s1;
     e[17] = rp2 * (-vymz + qymz) + s2;
     e[18] = rp0 * (+q0) + s0;
+    const C om = P.omega;
+    if (!GENERIC) {
+#pragma unroll
+        for (int d = 0; d < 18; ++d) y[d] = x[d] - om * (x[d] - e[d]);
+    } else {
     C fx = P.fx, fy = P.fy, fz = P.fz;
     if (P.force_mode == 1) { fx = P.fx * rho; fy = P.fy * rho; fz = P.fz * rho; }
-    const C om = P.omega;
     y[0] = x[0] - om * (x[0] - e[0]) + fx - fy;
     y[1] = x[1] - om * (x[1] - e[1]) + fx - fz;
     y[2] = x[2] - om * (x[2] - e[2]) + fx + fy;
@@ -165,6 +197,7 @@ __device__ __forceinline__ void bgk_collide(const C (&x)[19], C (&y)[19], const 
     y[15] = x[15] - om * (x[15] - e[15]) - fy - fz;
     y[16] = x[16] - om * (x[16] - e[16]) - fy;
     y[17] = x[17] - om * (x[17] - e[17]) - fy + fz;
+    }
     y[18] = x[18] - om * (x[18] - e[18]);
 }
 

@@ -45,6 +45,12 @@ template <class S, class C> struct SweepArgs {
     const int* obs;   // optional: obstacle mask, Fortran layout (1:l,1:m,1:n)
     long long obs_nx, obs_nxy;
     int imin, imax, jmin, jmax, kmin, kmax;
+    // launch geometry of the warp-segment mapping
+    long long align_base;  // (address of a[0]) / sizeof(S), mod 32
+    int nseg;              // 32-node segments per row
+    int nseg_aligned;      // 1 when every row starts on a segment boundary
+    uint32_t nrows;        // m * n
+    FastDiv div_seg, div_m;
 };
 
 // Equilibrium population p (0..4 -> 01..05) of the inflow face
@@ -71,56 +77,15 @@ __device__ __forceinline__ C roundtrip(C v, float scl, float inv) {
     return Conv<S, C>::ld(Conv<S, C>::st(v, scl), inv);
 }
 
-// Pull of population D at node (i,j,k) through the boundary rules above.
-template <class S, class C, int BC, int D>
-__device__ __forceinline__ C pull_general(const SweepArgs<S, C>& P, int i, int j, int k,
-                                          long long c, uint32_t solid_links) {
-    constexpr int cx = cx_of(D), cy = cy_of(D), cz = cz_of(D), od = opp_of(D);
-    int si = i - cx, sj = j - cy, sk = k - cz;
-    const bool ox = (cx == 1 && i == 1) || (cx == -1 && i == P.l);
-    const bool oy = (cy == 1 && j == 1) || (cy == -1 && j == P.m);
-    const bool oz = (cz == 1 && k == 1) || (cz == -1 && k == P.n);
-    const float inv = P.inv_scale;
-    if (BC == BC_DRIVEN) {
-        if (ox || oy || oz) {
-            C v = Conv<S, C>::ld(P.a[od][c], inv);
-            if (D == 1 && sk == P.n + 1) v = roundtrip<S, C>(v + P.lid_force, P.scale, inv);
-            if (D == 10 && sk == P.n + 1) v = roundtrip<S, C>(v - P.lid_force, P.scale, inv);
-            return v;
-        }
-    } else if (BC == BC_CHANNEL) {
-        if (oz) return Conv<S, C>::ld(P.a[od][c], inv);
-        if (ox) si = (cx == 1) ? P.l : 1;
-        if (oy) sj = (cy == 1) ? P.m : 1;
-    } else if (BC == BC_PERIODIC) {
-        if (ox) si = (cx == 1) ? P.l : 1;
-        if (oy) sj = (cy == 1) ? P.m : 1;
-        if (oz) sk = (cz == 1) ? P.n : 1;
-    } else if (BC == BC_INFLOW) {
-        if (cx == 1 && ox) {
-            if (D < 5) return roundtrip<S, C>(inflow_eq<C>(D, P.u_inflow, P.inflow_cte1, P.col), P.scale, inv);
-        }
-        if (oy) sj = (cy == 1) ? P.m : 1;
-        if (oz) sk = (cz == 1) ? P.n : 1;
-    }
-    if (!(ox || oy || oz) && ((solid_links >> D) & 1u)) return Conv<S, C>::ld(P.a[od][c], inv);
-    const long long s = (long long)si + P.nx * (long long)sj + P.nxy * (long long)sk;
-    if (D == 18) return Conv<S, C>::ld(P.a[18][s], inv);
-    return Conv<S, C>::ld(ldro<S>(P.a[D] + s), inv);
-}
-
-template <class S, class C, int BC, int D>
-struct PullAll {
-    __device__ __forceinline__ static void run(const SweepArgs<S, C>& P, int i, int j, int k,
-                                               long long c, uint32_t sl, C (&x)[19]) {
-        x[D] = pull_general<S, C, BC, D>(P, i, j, k, c, sl);
-        PullAll<S, C, BC, D + 1>::run(P, i, j, k, c, sl, x);
-    }
-};
-template <class S, class C, int BC>
-struct PullAll<S, C, BC, 19> {
-    __device__ __forceinline__ static void run(const SweepArgs<S, C>&, int, int, int, long long,
-                                               uint32_t, C (&)[19]) {}
+// Compile-time description of the six faces of a boundary case.
+template <int BC> struct Faces {
+    // periodic axes wrap; wall axes bounce back
+    static constexpr bool PX = (BC == BC_PERIODIC || BC == BC_CHANNEL);
+    static constexpr bool PY = (BC == BC_PERIODIC || BC == BC_CHANNEL || BC == BC_INFLOW);
+    static constexpr bool PZ = (BC == BC_PERIODIC || BC == BC_INFLOW);
+    static constexpr bool WX = (BC == BC_DRIVEN);
+    static constexpr bool WY = (BC == BC_DRIVEN);
+    static constexpr bool WZ = (BC == BC_DRIVEN || BC == BC_CHANNEL);
 };
 
 // Bit D set when the source x - c_D of node (i,j,k) is a solid node; bit 31
@@ -142,14 +107,29 @@ __device__ __forceinline__ uint32_t obstacle_links(const SweepArgs<S, C>& P, int
     return bits;
 }
 
-// One thread per interior node; blockDim = (TX, TY), grid = (ceil(l/TX), ceil(m/TY), n).
-template <class S, class C, int BC>
-__global__ void __launch_bounds__(256) sweep_ab_kernel(const SweepArgs<S, C> P) {
-    const int i = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int j = 1 + (int)(blockIdx.y * blockDim.y + threadIdx.y);
-    const int k = 1 + (int)blockIdx.z;
-    if (i > P.l || j > P.m) return;
-    const long long c = (long long)i + P.nx * (long long)j + P.nxy * (long long)k;
+// Warp-segment mapping: every warp owns 32 consecutive elements of one
+// (j, k) row whose first element is 32-element aligned in memory, whatever
+// the row's own alignment (P.align_base = (address of a[0]) / sizeof(S) mod
+// 32; a row starting mid-segment simply leaves lanes idle).  Aligned warps
+// make every store and every c_x = 0 load a whole number of 32-byte sectors.
+// One thread per node; blocks of 256 threads = 8 row segments.
+template <class S, class C, int BC, class IDX, bool GENERIC>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) sweep_ab_kernel(const SweepArgs<S, C> P) {
+    typedef Faces<BC> F;
+    const int lane = threadIdx.x & 31;
+    const uint32_t gw = blockIdx.x * 8u + (threadIdx.x >> 5);
+    const uint32_t row = P.div_seg.div(gw);
+    if (row >= P.nrows) return;
+    const int seg = (int)(gw - row * (uint32_t)P.nseg);
+    const uint32_t kk = P.div_m.div(row);
+    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
+    const int k = (int)kk + 1;
+    const IDX nx = (IDX)P.nx, nxy = (IDX)P.nxy;
+    const IDX rowoff = nx * (IDX)j + nxy * (IDX)k;
+    const int sh = (int)((P.align_base + (long long)rowoff + 1) & 31);
+    const int i = seg * 32 + lane + 1 - (P.nseg_aligned ? 0 : sh);
+    if (i < 1 || i > P.l) return;
+    const IDX c = rowoff + (IDX)i;
 
     uint32_t sl = 0;
     if (P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
@@ -157,23 +137,42 @@ __global__ void __launch_bounds__(256) sweep_ab_kernel(const SweepArgs<S, C> P) 
         sl = obstacle_links(P, i, j, k);
         if (sl & 0x80000000u) return;   // solid node: not updated
     }
-    const bool edge = (BC != BC_NONE) &&
-                      (i == 1 || i == P.l || j == 1 || j == P.m || k == 1 || k == P.n);
+    // source offsets for c = +1 (source at -1) and c = -1 (source at +1) on
+    // each axis; periodic axes wrap, others step into the halo (those links
+    // are then resolved below, never read from the halo)
+    const IDX oxm = (F::PX && i == 1) ? (IDX)(P.l - 1) : (IDX)(-1);
+    const IDX oxp = (F::PX && i == P.l) ? (IDX)(1 - P.l) : (IDX)1;
+    const IDX oym = (F::PY && j == 1) ? (IDX)(P.m - 1) * nx : -nx;
+    const IDX oyp = (F::PY && j == P.m) ? (IDX)(1 - P.m) * nx : nx;
+    const IDX ozm = (F::PZ && k == 1) ? (IDX)(P.n - 1) * nxy : -nxy;
+    const IDX ozp = (F::PZ && k == P.n) ? (IDX)(1 - P.n) * nxy : nxy;
+    const bool wxm = F::WX && i == 1, wxp = F::WX && i == P.l;
+    const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
+    const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
     const float inv = P.inv_scale;
     C x[19];
-    if (!edge && sl == 0) {
-        const long long nx = P.nx, nxy = P.nxy;
 #pragma unroll
-        for (int d = 0; d < 18; ++d) {
-            const long long s = c - cx_of(d) - cy_of(d) * nx - cz_of(d) * nxy;
-            x[d] = Conv<S, C>::ld(ldro<S>(P.a[d] + s), inv);
-        }
-        x[18] = Conv<S, C>::ld(P.a[18][c], inv);
-    } else {
-        PullAll<S, C, BC, 0>::run(P, i, j, k, c, sl, x);
+    for (int d = 0; d < 18; ++d) {
+        const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+        IDX off = c;
+        if (cx == 1) off += oxm; else if (cx == -1) off += oxp;
+        if (cy == 1) off += oym; else if (cy == -1) off += oyp;
+        if (cz == 1) off += ozm; else if (cz == -1) off += ozp;
+        bool bounce = ((sl >> d) & 1u) != 0;
+        if (cx == 1) bounce |= wxm; else if (cx == -1) bounce |= wxp;
+        if (cy == 1) bounce |= wym; else if (cy == -1) bounce |= wyp;
+        if (cz == 1) bounce |= wzm; else if (cz == -1) bounce |= wzp;
+        const S* src = bounce ? P.a[opp_of(d)] : P.a[d];
+        C v = Conv<S, C>::ld(ldro<S>(src + (bounce ? c : off)), inv);
+        if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
+            v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force, P.scale, inv);
+        if (BC == BC_INFLOW && cx == 1 && i == 1)
+            v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col), P.scale, inv);
+        x[d] = v;
     }
+    x[18] = Conv<S, C>::ld(P.a[18][c], inv);
     C y[19];
-    bgk_collide<C>(x, y, P.col);
+    bgk_collide<C, GENERIC>(x, y, P.col);
     const float scl = P.scale;
 #pragma unroll
     for (int d = 0; d < 18; ++d) P.b[d][c] = Conv<S, C>::st(y[d], scl);
