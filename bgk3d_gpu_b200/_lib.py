@@ -16,6 +16,7 @@ DROPIN_SP_PATH = os.path.join(PKG, "libbgk3d_dropin_sp.so")
 DROPIN_DP_PATH = os.path.join(PKG, "libbgk3d_dropin_dp.so")
 
 BGK_OK = 0
+BGK_ERR_ARG = -1
 KIND_F64, KIND_F32, KIND_F16, KIND_BF16, KIND_F32_F64 = 0, 1, 2, 3, 4
 BC_NONE, BC_DRIVEN, BC_PERIODIC, BC_CHANNEL, BC_INFLOW = -1, 0, 1, 2, 3
 PATTERN_AB, PATTERN_AA = 0, 1
@@ -71,6 +72,10 @@ def lib() -> ctypes.CDLL:
     L.bgk_reduce_workspace_bytes.restype = c_size_t
     L.bgk_moments.argtypes = [P, POINTER(c_void_p), c_void_p, c_void_p, c_size_t, c_void_p]
     L.bgk_moments.restype = c_int
+    L.bgk_moments_noalloc.argtypes = [P, POINTER(c_void_p), c_void_p, c_void_p]
+    L.bgk_moments_noalloc.restype = c_int
+    L.bgk_moments_noalloc_max_bytes.argtypes = []
+    L.bgk_moments_noalloc_max_bytes.restype = c_size_t
     L.bgk_draglift.argtypes = [P, POINTER(c_void_p), c_int, c_int, c_int, c_int, c_int, c_int,
                                c_void_p, c_void_p, c_size_t, c_void_p]
     L.bgk_draglift.restype = c_int

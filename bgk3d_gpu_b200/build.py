@@ -28,7 +28,7 @@ NVCC_FLAGS = ARCH + [
     "-I" + INCLUDE, "-I" + CSRC,
 ]
 
-LIB_SOURCES = ["bgk_api.cu", "lattice.cu"]
+LIB_SOURCES = ["bgk_api.cu", "lattice.cu", "noalloc.cu"]
 LIB = "libbgk3d_b200.so"
 DROPIN_SP = "libbgk3d_dropin_sp.so"
 DROPIN_DP = "libbgk3d_dropin_dp.so"

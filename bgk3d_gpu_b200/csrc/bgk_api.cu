@@ -207,6 +207,10 @@ int launch_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, i
 
 using namespace bgk;
 
+namespace bgk {
+int moments_launch(const bgk_sweep_params* p, void* const* a, double* out, double* ws, cudaStream_t st);
+}
+
 #define KIND_DISPATCH(kind, CALL)                                                     \
     switch (kind) {                                                                   \
         case K_F64: { typedef double S; typedef double C; return CALL; }              \
@@ -216,6 +220,10 @@ using namespace bgk;
         case K_F32_F64: { typedef float S; typedef double C; return CALL; }           \
     }                                                                                 \
     return set_error(BGK_ERR_ARG, "bad kind");
+
+int bgk::moments_launch(const bgk_sweep_params* p, void* const* a, double* out, double* ws, cudaStream_t st) {
+    KIND_DISPATCH(p->kind, (launch_moments<S, C>(p, a, out, ws, st)));
+}
 
 extern "C" {
 
@@ -256,8 +264,7 @@ int bgk_moments(const bgk_sweep_params* p, void* const* a, double* out_dev, void
     if (workspace_bytes < bgk_reduce_workspace_bytes(p->l, p->m, p->n))
         return set_error(BGK_ERR_ARG, "workspace too small: %zu < %zu", workspace_bytes,
                          bgk_reduce_workspace_bytes(p->l, p->m, p->n));
-    cudaStream_t st = (cudaStream_t)stream;
-    KIND_DISPATCH(p->kind, (launch_moments<S, C>(p, a, out_dev, (double*)workspace, st)));
+    return bgk::moments_launch(p, a, out_dev, (double*)workspace, (cudaStream_t)stream);
 }
 
 int bgk_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks, int ke,

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdarg>
 #include <cuda_runtime.h>
+#include "bgk3d_b200.h"
 
 namespace bgk {
 // Record a formatted message as the calling thread's last error; returns code.
@@ -10,4 +11,10 @@ int set_error(int code, const char* fmt, ...);
 int check_launch(const char* what);
 // Block shape for one-thread-per-node sweeps over (i, j) rows: TX x TY = 256.
 dim3 row_block(int l);
+// Parameter checks shared by every entry point (returns BGK_OK or an error).
+int validate(const struct bgk_sweep_params* p);
+// The two launches of the FP64 moments reduction, with the per-block
+// partials in ws (bgk_reduce_workspace_bytes(l, m, n) bytes).
+int moments_launch(const struct bgk_sweep_params* p, void* const* a, double* out, double* ws,
+                   cudaStream_t st);
 }  // namespace bgk

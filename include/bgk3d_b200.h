@@ -93,6 +93,20 @@ size_t bgk_reduce_workspace_bytes(int l, int m, int n);
 int bgk_moments(const bgk_sweep_params* p, void* const* a, double* out_dev, void* workspace,
                 size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of bgk_moments.  No counterpart in the reference:
+   for callers that cannot allocate device memory where they need the
+   diagnostic (a Fortran/OpenACC driver whose device memory is owned by the
+   directive runtime, a solver or server that reserves its whole memory budget
+   up front and forbids allocation in its time loop).  The per-block partial
+   sums live in a 2 MiB device array inside the library (bgk_moments_noalloc_
+   max_bytes()), held on every GPU that loads the library until exit; the
+   device address is looked up on the first call on each device (make that
+   call before any stream capture).  Lattices whose reduction needs more
+   scratch than that are rejected with BGK_ERR_ARG.  Calls share the array:
+   calls that overlap on the GPU race.  Results are identical to bgk_moments. */
+int bgk_moments_noalloc(const bgk_sweep_params* p, void* const* a, double* out_dev, void* stream);
+size_t bgk_moments_noalloc_max_bytes(void);
+
 /* FP64 momentum-exchange force (Fx, Fy, Fz, unnormalised) on the obstacle,
    summed over fluid nodes in the box [is..ie]x[js..je]x[ks..ke]
    (SRC/draglift.F90:77-176) into out_dev[0..2]. */
