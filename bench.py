@@ -139,18 +139,19 @@ def _barrier(ws: int):
         dist.barrier()
 
 
-def make_tgv_state(dev_lat):
+def tgv_host_state(kind_torch_dtype):
+    """TGV initial state in the reference layout (19, n+2, m+2, l+2), built on
+    the device with torch (set-up only) and returned in pinned host memory."""
     import torch
     from bgk3d_gpu_b200 import fields as F
     rho, ux, uy, uz = F.taylor_green_fields(L_, M_, N_, U0, device="cuda")
-    feq = F.equilibrium_shifted_torch(rho, ux, uy, uz, torch.float32)
+    feq = F.equilibrium_shifted_torch(rho, ux, uy, uz, kind_torch_dtype)
     del rho, ux, uy, uz
-    for d in range(19):
-        dev_lat._a[d][1:N_ + 1, 1:M_ + 1, 1:L_ + 1].copy_(feq[d])
-        if d < 18:
-            dev_lat._b[d].copy_(dev_lat._a[d])
+    host = torch.zeros((19, N_ + 2, M_ + 2, L_ + 2), dtype=kind_torch_dtype).pin_memory()
+    host[:, 1:N_ + 1, 1:M_ + 1, 1:L_ + 1].copy_(feq)
     del feq
     torch.cuda.synchronize()
+    return host
 
 
 def cpu_sample(seconds: float = 12.0, kind: int = 1):
@@ -236,10 +237,10 @@ def ref_cuda_glups(steps: int = 200):
     lib = ctypes.CDLL(path)
     lib.col_mc_gpu.argtypes = [ctypes.c_void_p] * 37 + [ctypes.c_int] * 5 + [ctypes.c_float] * 12
     lib.bcond_periodic_gpu.argtypes = [ctypes.POINTER(ctypes.c_void_p)] + [ctypes.c_int] * 5
-    from bgk3d_gpu_b200.lattice import DeviceLattice
-    lat = DeviceLattice(L_, M_, N_, kind="f32", bcase="periodic", omega=OMEGA)
-    make_tgv_state(lat)
-    a, b = list(lat._a), list(lat._b)
+    host = tgv_host_state(torch.float32)
+    A = host.cuda()
+    B = A[:18].clone()
+    a, b = [A[d] for d in range(19)], [B[d] for d in range(18)]
     nx, ny = L_ + 2, M_ + 2
 
     def step():
@@ -260,7 +261,7 @@ def ref_cuda_glups(steps: int = 200):
     e1.record(torch.cuda.default_stream())
     e1.synchronize()
     ms = e0.elapsed_time(e1)
-    del lat
+    del A, B, a, b
     torch.cuda.empty_cache()
     return L_ * M_ * N_ * steps / (ms * 1e-3) / 1e9
 
@@ -273,13 +274,14 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from bgk3d_gpu_b200 import _lib
-    from bgk3d_gpu_b200.lattice import DeviceLattice
-    lat = DeviceLattice(L_, M_, N_, kind="f32", bcase="periodic", omega=OMEGA)
-    make_tgv_state(lat)
+    from bgk3d_gpu_b200.lattice import Lattice
+    host = tgv_host_state(torch.float32)
+    lat = Lattice(L_, M_, N_, kind="f32", bcase="periodic", omega=OMEGA, pattern=args.pattern)
+    lat.upload(host.numpy())
     stream = torch.cuda.current_stream()
-    for _ in range(args.warmup):
-        lat.sweep()
+    # warm-up includes the capture of the 16-step CUDA graph (first run of >= 32 steps)
+    args.warmup = max(args.warmup, 32)
+    lat.step(args.warmup)
     torch.cuda.synchronize()
     _barrier(ws)
     clk = ClockSampler(local)
@@ -289,8 +291,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     _barrier(ws)
     e0.record(stream)
-    for _ in range(args.steps):
-        lat.sweep()
+    lat.step(args.steps)
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize()
@@ -302,6 +303,8 @@ def run_ours(args):
     launch_s = ms * 1e-3 / args.steps
     achieved = B_ALG_F32 * nodes / launch_s / 1e9
     peak, peak_src = _peaks()
+    if args.steps % 2:
+        lat.step(1)
     ke = lat.moments()
     if args.kernel_only:
         if rank == 0:
@@ -313,8 +316,10 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
     # ---- e2e through the reference-facing drop-in ABI with host buffers --------
-    e2e = run_e2e(lat, args)
+    lat.close()
     del lat
+    torch.cuda.empty_cache()
+    e2e = run_e2e(host, args)
     torch.cuda.empty_cache()
     ref_cuda = ref_cuda_glups() if rank == 0 else None
     if ws > 1:
@@ -331,13 +336,14 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (Taylor-Green vortex initial condition, BASELINE form)",
         "config": {"workload": WORKLOAD, "l": L_, "m": M_, "n": N_, "tau": TAU, "u0": U0,
-                   "pattern": "AB two-lattice, boundaries fused",
+                   "pattern": f"{args.pattern.upper()} (library-owned padded lattice, boundaries fused, CUDA graph)",
                    "l2": "inputs 2.6 GB > 126 MB L2 (no flush needed)",
                    "parallelism": f"replicas x{ws}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
                      "traffic": traffic, "b_alg_per_lup": B_ALG_F32,
-                     "kernel": "sweep_ab_kernel<float,float,PERIODIC>"},
+                     "kernel": "sweep_ab_kernel<float,float,PERIODIC,int,false>" if args.pattern == "ab"
+                     else "aa_odd_kernel + aa_even_kernel <float,float,PERIODIC,int,false>"},
         "cpu_baseline": {"value": cpu[0], "unit": "GLUPS", "cores": cpu[1], "kind": "port",
                          "sample": cpu[2]},
         "e2e": e2e,
@@ -350,7 +356,7 @@ def run_ours(args):
     return 0
 
 
-def run_e2e(lat, args):
+def run_e2e(host, args):
     """Same workload through the reference's C ABI (bcond_periodic_gpu + col_mc_gpu
     of libbgk3d_dropin_sp.so), from pinned host memory: H2D of the initial
     state, every step the FP64 kinetic-energy reduction read back to the host,
@@ -359,11 +365,10 @@ def run_e2e(lat, args):
     from bgk3d_gpu_b200 import _lib
     D = _lib.load_dropin(False)
     L = _lib.lib()
-    host = torch.stack([t for t in lat._a]).cpu().pin_memory()
     host_out = torch.empty_like(host).pin_memory()
     ke_host = torch.empty(5, dtype=torch.float64).pin_memory()
-    A = torch.empty_like(lat.A)
-    B = torch.empty_like(lat.B)
+    A = torch.empty(host.shape, dtype=host.dtype, device="cuda")
+    B = torch.empty((18,) + tuple(host.shape[1:]), dtype=host.dtype, device="cuda")
     a = [A[d] for d in range(19)]
     b = [B[d] for d in range(18)]
     nx, ny = L_ + 2, M_ + 2
@@ -412,6 +417,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--lattice", type=int, nargs=3, default=None, metavar=("L", "M", "N"),
                     help="override the lattice extents (profiling runs of a smaller case)")
+    ap.add_argument("--pattern", default="ab", choices=["ab", "aa"],
+                    help="two-lattice (ab) or in-place (aa) streaming")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the sweep only (no e2e, CPU or reference-CUDA legs): for ncu captures")
     args = ap.parse_args()

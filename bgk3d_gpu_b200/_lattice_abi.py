@@ -1,0 +1,46 @@
+"""ctypes signatures of the library-owned lattice entry points (include/bgk3d_lattice.h)."""
+from __future__ import annotations
+
+from ctypes import (POINTER, Structure, c_double, c_float, c_int, c_longlong, c_size_t, c_void_p)
+
+
+class LatticeDesc(Structure):
+    """Mirror of bgk_lattice_desc."""
+    _fields_ = [
+        ("kind", c_int), ("bcase", c_int), ("pattern", c_int),
+        ("l", c_int), ("m", c_int), ("n", c_int),
+        ("omega", c_double),
+        ("force_mode", c_int), ("fx", c_double), ("fy", c_double), ("fz", c_double),
+        ("lid_force", c_double), ("u_inflow", c_double),
+        ("scale", c_float),
+    ]
+
+
+def bind(L) -> None:
+    D = POINTER(LatticeDesc)
+    L.bgk_lattice_desc_init.argtypes = [D, c_int, c_int, c_int, c_int, c_int, c_double]
+    L.bgk_lattice_desc_init.restype = None
+    L.bgk_lattice_device_bytes.argtypes = [D]
+    L.bgk_lattice_device_bytes.restype = c_size_t
+    L.bgk_lattice_create.argtypes = [D, POINTER(c_void_p)]
+    L.bgk_lattice_create.restype = c_int
+    L.bgk_lattice_destroy.argtypes = [c_void_p]
+    L.bgk_lattice_destroy.restype = c_int
+    L.bgk_lattice_set_obstacle.argtypes = [c_void_p, c_void_p]
+    L.bgk_lattice_set_obstacle.restype = c_int
+    L.bgk_lattice_load.argtypes = [c_void_p, c_void_p, c_void_p]
+    L.bgk_lattice_load.restype = c_int
+    L.bgk_lattice_store.argtypes = [c_void_p, c_void_p, c_void_p]
+    L.bgk_lattice_store.restype = c_int
+    L.bgk_lattice_step.argtypes = [c_void_p, c_int, c_void_p]
+    L.bgk_lattice_step.restype = c_int
+    L.bgk_lattice_set_omega.argtypes = [c_void_p, c_double]
+    L.bgk_lattice_set_omega.restype = c_int
+    L.bgk_lattice_moments.argtypes = [c_void_p, c_void_p, c_void_p]
+    L.bgk_lattice_moments.restype = c_int
+    L.bgk_lattice_draglift.argtypes = [c_void_p] + [c_int] * 6 + [c_void_p, c_void_p]
+    L.bgk_lattice_draglift.restype = c_int
+    L.bgk_lattice_steps.argtypes = [c_void_p]
+    L.bgk_lattice_steps.restype = c_longlong
+    L.bgk_lattice_arrays.argtypes = [c_void_p, POINTER(c_void_p), POINTER(c_longlong), POINTER(c_longlong)]
+    L.bgk_lattice_arrays.restype = c_int

@@ -9,6 +9,7 @@
 #include "bgk_internal.h"
 #include "sweep_ab.cuh"
 #include "reduce.cuh"
+#include "host_args.cuh"
 
 namespace bgk {
 
@@ -64,58 +65,6 @@ int validate(const bgk_sweep_params* p) {
     return BGK_OK;
 }
 
-template <class C>
-ColConst<C> col_const(const bgk_sweep_params* p) {
-    ColConst<C> k;
-    k.omega = (C)p->omega; k.cte0 = (C)p->cte0; k.cte1 = (C)p->cte1;
-    k.p0 = (C)p->p0; k.p1 = (C)p->p1; k.p2 = (C)p->p2;
-    k.rf = (C)p->rf; k.qf = (C)p->qf; k.tre = (C)p->tre;
-    k.force_mode = p->force_mode;
-    k.fx = (C)p->fx; k.fy = (C)p->fy; k.fz = (C)p->fz;
-    return k;
-}
-
-template <class S, class C>
-SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* const* b) {
-    SweepArgs<S, C> A;
-    for (int d = 0; d < 19; ++d) {
-        A.a[d] = (const S*)a[d];
-        A.b[d] = (d < 18) ? (S*)b[d] : (S*)a[18];
-    }
-    A.nx = p->nx; A.nxy = p->nx * p->ny;
-    A.l = p->l; A.m = p->m; A.n = p->n;
-    A.col = col_const<C>(p);
-    A.lid_force = (C)p->lid_force;
-    A.u_inflow = (C)p->u_inflow;
-    A.inflow_cte1 = (C)p->inflow_cte1;
-    A.scale = (p->kind == K_F16 || p->kind == K_BF16) ? p->scale : 1.0f;
-    A.inv_scale = 1.0f / A.scale;
-    const bool has_obs = p->obs && p->imin <= p->imax && p->jmin <= p->jmax && p->kmin <= p->kmax;
-    A.obs = has_obs ? p->obs : nullptr;
-    A.obs_nx = p->obs_nx; A.obs_nxy = (long long)p->obs_nx * p->obs_ny;
-    A.imin = p->imin; A.imax = p->imax; A.jmin = p->jmin; A.jmax = p->jmax;
-    A.kmin = p->kmin; A.kmax = p->kmax;
-    return A;
-}
-
-// Warp-segment launch geometry of sweep_ab_kernel (see sweep_ab.cuh).
-template <class S, class C>
-void segment_geometry(SweepArgs<S, C>& A, const void* a0) {
-    const long long elem = (long long)((uintptr_t)a0 / sizeof(S));
-    A.align_base = elem & 31;
-    const bool aligned = ((A.align_base + 1) % 32 == 0) && (A.nx % 32 == 0);
-    A.nseg_aligned = aligned ? 1 : 0;
-    A.nseg = aligned ? (A.l + 31) / 32 : (A.l + 62) / 32;
-    A.nrows = (uint32_t)((long long)A.m * A.n);
-    A.div_seg.init((uint32_t)A.nseg);
-    A.div_m.init((uint32_t)A.m);
-}
-
-// True unless the collision can use the shifted, force-free specialisation.
-bool generic_collision(const bgk_sweep_params* p) {
-    return !(p->cte1 == 1.0 && p->cte0 == 0.0 && p->fx == 0.0 && p->fy == 0.0 && p->fz == 0.0);
-}
-
 template <class S, class C, int BC>
 void launch_sweep_bc(const SweepArgs<S, C>& A, long long nelem, unsigned blocks, bool generic,
                      cudaStream_t st) {
@@ -151,22 +100,6 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, cuda
         case BC_INFLOW: launch_sweep_bc<S, C, BC_INFLOW>(A, nelem, nb, g, st); break;
     }
     return check_launch("sweep_ab_kernel");
-}
-
-template <class S, class C>
-FieldArgs<S, C> field_args(const bgk_sweep_params* p, void* const* a) {
-    FieldArgs<S, C> F;
-    for (int d = 0; d < 19; ++d) F.a[d] = (const S*)a[d];
-    F.nx = p->nx; F.nxy = p->nx * p->ny;
-    F.l = p->l; F.m = p->m; F.n = p->n;
-    F.cte1 = (C)p->cte1;
-    F.inv_scale = (p->kind == K_F16 || p->kind == K_BF16) ? 1.0f / p->scale : 1.0f;
-    const bool has_obs = p->obs && p->imin <= p->imax && p->jmin <= p->jmax && p->kmin <= p->kmax;
-    F.obs = has_obs ? p->obs : nullptr;
-    F.obs_nx = p->obs_nx; F.obs_nxy = (long long)p->obs_nx * p->obs_ny;
-    F.imin = p->imin; F.imax = p->imax; F.jmin = p->jmin; F.jmax = p->jmax;
-    F.kmin = p->kmin; F.kmax = p->kmax;
-    return F;
 }
 
 // Grid of the moments pass: rows of the (i, j) plane x KB blocks striding k.
@@ -207,10 +140,6 @@ int launch_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, i
 
 using namespace bgk;
 
-namespace bgk {
-int moments_launch(const bgk_sweep_params* p, void* const* a, double* out, double* ws, cudaStream_t st);
-}
-
 #define KIND_DISPATCH(kind, CALL)                                                     \
     switch (kind) {                                                                   \
         case K_F64: { typedef double S; typedef double C; return CALL; }              \
@@ -223,6 +152,15 @@ int moments_launch(const bgk_sweep_params* p, void* const* a, double* out, doubl
 
 int bgk::moments_launch(const bgk_sweep_params* p, void* const* a, double* out, double* ws, cudaStream_t st) {
     KIND_DISPATCH(p->kind, (launch_moments<S, C>(p, a, out, ws, st)));
+}
+
+int bgk::sweep_launch(const bgk_sweep_params* p, void* const* a, void* const* b, cudaStream_t st) {
+    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, st)));
+}
+
+int bgk::draglift_launch(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
+                         int ke, double* out, double* ws, size_t ws_bytes, cudaStream_t st) {
+    KIND_DISPATCH(p->kind, (launch_draglift<S, C>(p, a, is, ie, js, je, ks, ke, out, ws, ws_bytes, st)));
 }
 
 extern "C" {
@@ -246,8 +184,7 @@ int bgk_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, void* s
     if (!a || !b) return set_error(BGK_ERR_ARG, "null population pointer array");
     for (int d = 0; d < 19; ++d)
         if (!a[d] || (d < 18 && !b[d])) return set_error(BGK_ERR_ARG, "null population %d", d + 1);
-    cudaStream_t st = (cudaStream_t)stream;
-    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, st)));
+    return bgk::sweep_launch(p, a, b, (cudaStream_t)stream);
 }
 
 size_t bgk_reduce_workspace_bytes(int l, int m, int n) {
@@ -272,9 +209,8 @@ int bgk_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int 
     if (int e = validate(p)) return e;
     if (!a || !out_dev || !workspace) return set_error(BGK_ERR_ARG, "null pointer");
     if (ie < is || je < js || ke < ks) return set_error(BGK_ERR_ARG, "empty draglift box");
-    cudaStream_t st = (cudaStream_t)stream;
-    KIND_DISPATCH(p->kind, (launch_draglift<S, C>(p, a, is, ie, js, je, ks, ke, out_dev, (double*)workspace,
-                                                  workspace_bytes, st)));
+    return bgk::draglift_launch(p, a, is, ie, js, je, ks, ke, out_dev, (double*)workspace, workspace_bytes,
+                                (cudaStream_t)stream);
 }
 
 int bgk_device_sync(void) {

@@ -17,4 +17,9 @@ int validate(const struct bgk_sweep_params* p);
 // partials in ws (bgk_reduce_workspace_bytes(l, m, n) bytes).
 int moments_launch(const struct bgk_sweep_params* p, void* const* a, double* out, double* ws,
                    cudaStream_t st);
+// The fused sweep launch(es) without argument validation.
+int sweep_launch(const struct bgk_sweep_params* p, void* const* a, void* const* b, cudaStream_t st);
+// The two launches of the FP64 drag/lift reduction.
+int draglift_launch(const struct bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
+                    int ke, double* out, double* ws, size_t ws_bytes, cudaStream_t st);
 }  // namespace bgk

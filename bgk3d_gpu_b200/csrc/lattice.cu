@@ -1,0 +1,395 @@
+// Library-owned lattices (include/bgk3d_lattice.h): padded aligned layout,
+// AB and in-place AA time steps, CUDA-graph replay of long step runs,
+// host transfers in the reference layout, FP64 diagnostics.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+#include "bgk3d_b200.h"
+#include "bgk3d_lattice.h"
+#include "bgk_internal.h"
+#include "host_args.cuh"
+#include "sweep_aa.cuh"
+
+using namespace bgk;
+
+struct bgk_lattice {
+    bgk_lattice_desc desc;
+    bgk_sweep_params p;          // sweep parameters (kind, case, constants, layout, obstacle)
+    int es;                      // bytes per stored value
+    long long nx, ny, nz, origin, plane;   // elements
+    char* base = nullptr;
+    size_t bytes = 0;
+    std::vector<void*> planes;   // plane pointers at element (0,0,0)
+    void* a[19];                 // AB: current populations; AA: slot arrays
+    void* b[19];                 // AB: next populations (b[18] = a[18])
+    int32_t* obs_dev = nullptr;
+    long long steps = 0;
+    double* ws = nullptr;
+    size_t ws_bytes = 0;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+};
+
+namespace {
+
+constexpr int kGraphSteps = 16;
+
+int elem_bytes(int kind) {
+    switch (kind) {
+        case K_F64: return 8;
+        case K_F32: case K_F32_F64: return 4;
+        default: return 2;
+    }
+}
+
+struct Geometry { long long nx, ny, nz, origin, plane; };
+
+Geometry geometry(const bgk_lattice_desc* d) {
+    Geometry g;
+    g.nx = ((long long)d->l + 2 + 31) / 32 * 32;   // row pitch: whole 32-element segments
+    g.ny = (long long)d->m + 2;
+    g.nz = (long long)d->n + 2;
+    g.origin = 31;                                   // node (1, j, k) on a segment boundary
+    const long long raw = g.nx * g.ny * g.nz + g.origin + 32;
+    const long long unit = 256 / elem_bytes(d->kind); // plane starts on 256-byte boundaries
+    g.plane = (raw + unit - 1) / unit * unit;
+    return g;
+}
+
+int nplanes(const bgk_lattice_desc* d) { return d->pattern == BGK_PATTERN_AA ? 19 : 37; }
+
+void drop_graph(bgk_lattice* L) {
+    if (L->graph) cudaGraphExecDestroy(L->graph);
+    L->graph = nullptr;
+    L->graph_steps = 0;
+}
+
+template <class S, class C, int BC>
+void launch_aa_bc(const SweepArgs<S, C>& A, bool odd, bool generic, long long nelem, unsigned blocks,
+                  cudaStream_t st) {
+    if (nelem < (1LL << 31)) {
+        if (odd) {
+            if (generic) aa_odd_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
+            else aa_odd_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
+        } else {
+            if (generic) aa_even_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
+            else aa_even_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
+        }
+    } else {
+        if (odd) aa_odd_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
+        else aa_even_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
+    }
+}
+
+template <class S, class C>
+int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, cudaStream_t st) {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, slots, slots);
+    A.b[18] = (S*)slots[18];
+    segment_geometry(A, slots[0]);
+    const long long warps = (long long)A.nseg * p->m * p->n;
+    if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
+    const unsigned blocks = (unsigned)((warps + 7) / 8);
+    const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
+    const bool g = generic_collision(p);
+    switch (p->bcase) {
+        case BC_DRIVEN: launch_aa_bc<S, C, BC_DRIVEN>(A, odd, g, nelem, blocks, st); break;
+        case BC_PERIODIC: launch_aa_bc<S, C, BC_PERIODIC>(A, odd, g, nelem, blocks, st); break;
+        case BC_CHANNEL: launch_aa_bc<S, C, BC_CHANNEL>(A, odd, g, nelem, blocks, st); break;
+        case BC_INFLOW: launch_aa_bc<S, C, BC_INFLOW>(A, odd, g, nelem, blocks, st); break;
+        default: return set_error(BGK_ERR_ARG, "AA lattices need a boundary case");
+    }
+    return check_launch(odd ? "aa_odd_kernel" : "aa_even_kernel");
+}
+
+template <class S, class C>
+int launch_aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, slots, slots);
+    dim3 blk(128), grd((p->m + 127) / 128, p->n);
+    aa_outflow_prepass_kernel<S, C><<<grd, blk, 0, st>>>(A);
+    return check_launch("aa_outflow_prepass_kernel");
+}
+
+#define LKIND_DISPATCH(kind, CALL)                                                  \
+    switch (kind) {                                                                 \
+        case K_F64: { typedef double S; typedef double C; return CALL; }            \
+        case K_F32: { typedef float S; typedef float C; return CALL; }              \
+        case K_F16: { typedef __half S; typedef float C; return CALL; }             \
+        case K_BF16: { typedef __nv_bfloat16 S; typedef float C; return CALL; }     \
+        case K_F32_F64: { typedef float S; typedef double C; return CALL; }         \
+    }                                                                               \
+    return set_error(BGK_ERR_ARG, "bad kind");
+
+int aa_step(const bgk_sweep_params* p, void* const* slots, bool odd, cudaStream_t st) {
+    LKIND_DISPATCH(p->kind, (launch_aa<S, C>(p, slots, odd, st)));
+}
+
+int aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
+    LKIND_DISPATCH(p->kind, (launch_aa_prepass<S, C>(p, slots, st)));
+}
+
+// AA: population p of the observable state lives in slot opp(p).
+void observable(const bgk_lattice* L, void** out) {
+    if (L->desc.pattern == BGK_PATTERN_AA)
+        for (int d = 0; d < 19; ++d) out[d] = L->a[opp_of(d)];
+    else
+        for (int d = 0; d < 19; ++d) out[d] = L->a[d];
+}
+
+// One time step on stream st (no graph).
+int one_step(bgk_lattice* L, cudaStream_t st) {
+    if (L->desc.pattern == BGK_PATTERN_AA) {
+        const bool odd = (L->steps % 2) == 0;   // Layout E -> odd kernel
+        if (int e = aa_step(&L->p, L->a, odd, st)) return e;
+    } else {
+        if (int e = sweep_launch(&L->p, L->a, L->b, st)) return e;
+        for (int d = 0; d < 18; ++d) std::swap(L->a[d], L->b[d]);
+    }
+    ++L->steps;
+    return BGK_OK;
+}
+
+// Capture kGraphSteps steps (starting from an even step count, so the
+// pointer arrangement / slot layout after the graph equals the one before).
+int build_graph(bgk_lattice* L) {
+    if (!L->cap_stream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&L->cap_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "stream create: %s", cudaGetErrorString(e));
+    }
+    const long long saved = L->steps;
+    void* a0[19]; void* b0[19];
+    std::memcpy(a0, L->a, sizeof a0); std::memcpy(b0, L->b, sizeof b0);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(L->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    int rc = BGK_OK;
+    for (int s = 0; s < kGraphSteps && rc == BGK_OK; ++s) rc = one_step(L, L->cap_stream);
+    e = cudaStreamEndCapture(L->cap_stream, &g);
+    L->steps = saved;
+    std::memcpy(L->a, a0, sizeof a0); std::memcpy(L->b, b0, sizeof b0);
+    if (rc != BGK_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&L->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { L->graph = nullptr; return set_error(BGK_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    L->graph_steps = kGraphSteps;
+    return BGK_OK;
+}
+
+int ensure_workspace(const bgk_lattice* Lc) {
+    bgk_lattice* L = const_cast<bgk_lattice*>(Lc);
+    const size_t need = std::max<size_t>(bgk_reduce_workspace_bytes(L->desc.l, L->desc.m, L->desc.n), 1 << 16);
+    if (L->ws && L->ws_bytes >= need) return BGK_OK;
+    if (L->ws) cudaFree(L->ws);
+    L->ws = nullptr;
+    cudaError_t e = cudaMalloc(&L->ws, need);
+    if (e != cudaSuccess) return set_error(BGK_ERR_NOMEM, "workspace: %s", cudaGetErrorString(e));
+    L->ws_bytes = need;
+    return BGK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void bgk_lattice_desc_init(bgk_lattice_desc* d, int kind, int bcase, int l, int m, int n, double omega) {
+    std::memset(d, 0, sizeof *d);
+    d->kind = kind; d->bcase = bcase; d->pattern = BGK_PATTERN_AB;
+    d->l = l; d->m = m; d->n = n; d->omega = omega;
+    d->scale = 1.0f;
+}
+
+size_t bgk_lattice_device_bytes(const bgk_lattice_desc* d) {
+    const Geometry g = geometry(d);
+    return (size_t)g.plane * nplanes(d) * elem_bytes(d->kind);
+}
+
+int bgk_lattice_create(const bgk_lattice_desc* d, bgk_lattice** out) {
+    if (!d || !out) return set_error(BGK_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (d->bcase < BC_DRIVEN || d->bcase > BC_INFLOW) return set_error(BGK_ERR_ARG, "lattices need a boundary case");
+    if (d->pattern != BGK_PATTERN_AB && d->pattern != BGK_PATTERN_AA) return set_error(BGK_ERR_ARG, "bad pattern");
+    bgk_lattice* L = new (std::nothrow) bgk_lattice;
+    if (!L) return set_error(BGK_ERR_NOMEM, "host allocation");
+    L->desc = *d;
+    const Geometry g = geometry(d);
+    L->nx = g.nx; L->ny = g.ny; L->nz = g.nz; L->origin = g.origin; L->plane = g.plane;
+    L->es = elem_bytes(d->kind);
+    bgk_sweep_params_init(&L->p, d->kind, d->l, d->m, d->n, d->omega);
+    L->p.bcase = d->bcase;
+    L->p.nx = g.nx; L->p.ny = g.ny;
+    L->p.force_mode = d->force_mode; L->p.fx = d->fx; L->p.fy = d->fy; L->p.fz = d->fz;
+    L->p.lid_force = d->lid_force; L->p.u_inflow = d->u_inflow; L->p.inflow_cte1 = 0.0;
+    L->p.scale = d->scale;
+    if (int e = validate(&L->p)) { delete L; return e; }
+    L->bytes = bgk_lattice_device_bytes(d);
+    cudaError_t e = cudaMalloc(&L->base, L->bytes);
+    if (e != cudaSuccess) {
+        delete L;
+        return set_error(BGK_ERR_NOMEM, "lattice of %zu bytes: %s", (size_t)bgk_lattice_device_bytes(d),
+                         cudaGetErrorString(e));
+    }
+    cudaMemset(L->base, 0, L->bytes);
+    const int np = nplanes(d);
+    L->planes.resize(np);
+    for (int q = 0; q < np; ++q) L->planes[q] = L->base + ((size_t)q * L->plane + L->origin) * L->es;
+    for (int q = 0; q < 19; ++q) L->a[q] = L->planes[q];
+    if (d->pattern == BGK_PATTERN_AB) {
+        for (int q = 0; q < 18; ++q) L->b[q] = L->planes[19 + q];
+        L->b[18] = L->a[18];
+    } else {
+        for (int q = 0; q < 19; ++q) L->b[q] = L->a[q];
+    }
+    *out = L;
+    return BGK_OK;
+}
+
+int bgk_lattice_destroy(bgk_lattice* L) {
+    if (!L) return BGK_OK;
+    drop_graph(L);
+    if (L->cap_stream) cudaStreamDestroy(L->cap_stream);
+    if (L->base) cudaFree(L->base);
+    if (L->obs_dev) cudaFree(L->obs_dev);
+    if (L->ws) cudaFree(L->ws);
+    delete L;
+    return BGK_OK;
+}
+
+int bgk_lattice_set_obstacle(bgk_lattice* L, const int32_t* obs) {
+    if (!L) return set_error(BGK_ERR_ARG, "null lattice");
+    drop_graph(L);
+    if (L->obs_dev) { cudaFree(L->obs_dev); L->obs_dev = nullptr; }
+    L->p.obs = nullptr;
+    L->p.imin = 1; L->p.imax = 0; L->p.jmin = 1; L->p.jmax = 0; L->p.kmin = 1; L->p.kmax = 0;
+    if (!obs) return BGK_OK;
+    const int l = L->desc.l, m = L->desc.m, n = L->desc.n;
+    int b[6] = {l + 1, 0, m + 1, 0, n + 1, 0};
+    for (int k = 1; k <= n; ++k)
+        for (int j = 1; j <= m; ++j)
+            for (int i = 1; i <= l; ++i)
+                if (obs[(size_t)(i - 1) + (size_t)l * (j - 1) + (size_t)l * m * (k - 1)] == 1) {
+                    b[0] = std::min(b[0], i); b[1] = std::max(b[1], i);
+                    b[2] = std::min(b[2], j); b[3] = std::max(b[3], j);
+                    b[4] = std::min(b[4], k); b[5] = std::max(b[5], k);
+                }
+    if (b[1] == 0) return BGK_OK;   // no solid node
+    bgk_sweep_params q = L->p;
+    q.obs = obs; q.obs_nx = l; q.obs_ny = m;
+    q.imin = b[0]; q.imax = b[1]; q.jmin = b[2]; q.jmax = b[3]; q.kmin = b[4]; q.kmax = b[5];
+    if (int e = validate(&q)) return e;
+    const size_t nb = (size_t)l * m * n * sizeof(int32_t);
+    cudaError_t e = cudaMalloc(&L->obs_dev, nb);
+    if (e != cudaSuccess) return set_error(BGK_ERR_NOMEM, "obstacle mask: %s", cudaGetErrorString(e));
+    e = cudaMemcpy(L->obs_dev, obs, nb, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "obstacle copy: %s", cudaGetErrorString(e));
+    q.obs = L->obs_dev;
+    L->p = q;
+    return BGK_OK;
+}
+
+int bgk_lattice_load(bgk_lattice* L, const void* host, void* stream) {
+    if (!L || !host) return set_error(BGK_ERR_ARG, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int l = L->desc.l, m = L->desc.m, n = L->desc.n;
+    const size_t es = L->es, row = (size_t)(l + 2) * es, rows = (size_t)(m + 2) * (n + 2);
+    // AB: reset the pointer arrangement to the base planes
+    for (int q = 0; q < 19; ++q) L->a[q] = L->planes[q];
+    if (L->desc.pattern == BGK_PATTERN_AB) {
+        for (int q = 0; q < 18; ++q) L->b[q] = L->planes[19 + q];
+        L->b[18] = L->a[18];
+    }
+    for (int d = 0; d < 19; ++d) {
+        void* dst = (L->desc.pattern == BGK_PATTERN_AA) ? L->a[opp_of(d)] : L->a[d];
+        const char* src = (const char*)host + (size_t)d * row * rows;
+        cudaError_t e = cudaMemcpy2DAsync(dst, (size_t)L->nx * es, src, row, row, rows, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "load: %s", cudaGetErrorString(e));
+    }
+    L->steps = 0;
+    if (L->desc.pattern == BGK_PATTERN_AA && L->desc.bcase == BC_INFLOW)
+        if (int e = aa_prepass(&L->p, L->a, st)) return e;
+    return BGK_OK;
+}
+
+int bgk_lattice_store(const bgk_lattice* L, void* host, void* stream) {
+    if (!L || !host) return set_error(BGK_ERR_ARG, "null argument");
+    if (L->desc.pattern == BGK_PATTERN_AA && (L->steps % 2) != 0)
+        return set_error(BGK_ERR_STATE, "AA lattice after an odd number of steps holds no observable state");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int l = L->desc.l, m = L->desc.m, n = L->desc.n;
+    const size_t es = L->es, row = (size_t)(l + 2) * es, rows = (size_t)(m + 2) * (n + 2);
+    void* obsv[19];
+    observable(L, obsv);
+    for (int d = 0; d < 19; ++d) {
+        char* dst = (char*)host + (size_t)d * row * rows;
+        cudaError_t e = cudaMemcpy2DAsync(dst, row, obsv[d], (size_t)L->nx * es, row, rows, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "store: %s", cudaGetErrorString(e));
+    }
+    return BGK_OK;
+}
+
+int bgk_lattice_step(bgk_lattice* L, int nsteps, void* stream) {
+    if (!L || nsteps < 0) return set_error(BGK_ERR_ARG, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int left = nsteps;
+    if (left >= 2 * kGraphSteps) {
+        if ((L->steps % 2) != 0) {   // reach the base arrangement first
+            if (int e = one_step(L, st)) return e;
+            --left;
+        }
+        if (!L->graph)
+            if (int e = build_graph(L)) return e;
+        while (left >= L->graph_steps) {
+            cudaError_t e = cudaGraphLaunch(L->graph, st);
+            if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+            L->steps += L->graph_steps;
+            left -= L->graph_steps;
+        }
+    }
+    while (left-- > 0)
+        if (int e = one_step(L, st)) return e;
+    return BGK_OK;
+}
+
+int bgk_lattice_set_omega(bgk_lattice* L, double omega) {
+    if (!L) return set_error(BGK_ERR_ARG, "null lattice");
+    drop_graph(L);
+    L->p.omega = omega;
+    L->desc.omega = omega;
+    return BGK_OK;
+}
+
+int bgk_lattice_moments(const bgk_lattice* L, double* out_dev, void* stream) {
+    if (!L || !out_dev) return set_error(BGK_ERR_ARG, "null argument");
+    if (L->desc.pattern == BGK_PATTERN_AA && (L->steps % 2) != 0)
+        return set_error(BGK_ERR_STATE, "AA lattice after an odd number of steps holds no observable state");
+    if (int e = ensure_workspace(L)) return e;
+    void* obsv[19];
+    observable(L, obsv);
+    return moments_launch(&L->p, obsv, out_dev, L->ws, (cudaStream_t)stream);
+}
+
+int bgk_lattice_draglift(const bgk_lattice* L, int is, int ie, int js, int je, int ks, int ke, double* out_dev,
+                         void* stream) {
+    if (!L || !out_dev) return set_error(BGK_ERR_ARG, "null argument");
+    if (L->desc.pattern == BGK_PATTERN_AA && (L->steps % 2) != 0)
+        return set_error(BGK_ERR_STATE, "AA lattice after an odd number of steps holds no observable state");
+    if (ie < is || je < js || ke < ks) return set_error(BGK_ERR_ARG, "empty draglift box");
+    if (int e = ensure_workspace(L)) return e;
+    void* obsv[19];
+    observable(L, obsv);
+    return draglift_launch(&L->p, obsv, is, ie, js, je, ks, ke, out_dev, L->ws, L->ws_bytes, (cudaStream_t)stream);
+}
+
+long long bgk_lattice_steps(const bgk_lattice* L) { return L ? L->steps : -1; }
+
+int bgk_lattice_arrays(const bgk_lattice* L, void** a19, long long* nx, long long* ny) {
+    if (!L || !a19) return set_error(BGK_ERR_ARG, "null argument");
+    observable(L, a19);
+    if (nx) *nx = L->nx;
+    if (ny) *ny = L->ny;
+    return BGK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,224 @@
+// In-place AA-pattern time step: one population set, half the footprint of
+// the two-lattice scheme, same arithmetic and the same boundary semantics as
+// sweep_ab_kernel (so the results are bit-identical to the reference's).
+//
+// Slot convention.  "Layout E" (after the even kernel): slot opp(p) of node x
+// holds the post-collision population p of x.  The odd kernel reads every
+// incoming population from its source node's slot opp(p) (or resolves it by
+// the boundary rules), collides, and pushes each outgoing population p to
+// slot p of its target node x + c_p ("Layout O": slot p of x then holds the
+// value x pulls in the next step).  The even kernel reads slot p of its own
+// node, collides, and writes population p into slot opp(p): purely local.
+// A thread's reads and writes touch the same memory locations, so neither
+// kernel has an inter-thread hazard.
+//
+// Boundaries in the odd kernel, link by link (same precedence as the AB sweep):
+//   * wall / solid source        -> read own slot p (= own post-collision opp(p));
+//     the mirrored outgoing link writes own slot opp(p) (lid: +-force, rounded
+//     through storage, on pops 02/11 at the top face);
+//   * periodic axes              -> read/push the wrapped node;
+//   * inflow face (x = 0)        -> constant equilibrium in; the node also
+//     writes that constant into its own slots 01..05 for the next even step;
+//     outgoing populations leaving through x = 0 are dropped;
+//   * outflow face (x = l+1)     -> read the halo cell's slot opp(p), which the
+//     even kernel (or the upload prepass) filled with the outflow equilibrium
+//     of node (l, j, k); the odd kernel of node (l, j, k) pushes the new
+//     outflow equilibrium into slots 10..14 of (l, j+c_y, k+c_z) (y/z wrapped).
+// Solid nodes are skipped by both kernels.  The observable (post-collision)
+// state exists only in Layout E, i.e. after an even number of steps.
+#pragma once
+#include "sweep_ab.cuh"
+
+namespace bgk {
+
+// Outflow equilibria e = 9..13 (pops 10..14) from the stored populations
+// a[] of node (l, j, k) at rho = 1 (SRC/bcond.inflow.F90:135-162).
+template <class C>
+__device__ __forceinline__ void outflow_eq(const C (&a)[19], C cte1, const ColConst<C>& K, C (&eq)[5]) {
+    const C rhoinv = C(1), crho = C(1), rf = K.rf, qf = K.qf, three = C(3), p1 = K.p1, p2 = K.p2;
+    const C xj = (a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13]) * rhoinv;
+    const C yj = (a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17]) * rhoinv;
+    const C zj = (a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15]) * rhoinv;
+    const C cvsq = xj * xj + yj * yj + zj * zj;
+    const C cx10 = rf * (-xj - yj) + qf * (three * (xj + yj) * (xj + yj) - cvsq);
+    const C cx11 = rf * (-xj - zj) + qf * (three * (xj + zj) * (xj + zj) - cvsq);
+    const C cx12 = rf * (-xj + yj) + qf * (three * (xj - yj) * (xj - yj) - cvsq);
+    const C cx13 = rf * (-xj + zj) + qf * (three * (xj - zj) * (xj - zj) - cvsq);
+    const C cx14 = rf * (-xj) + qf * (three * (xj) * (xj) - cvsq);
+    eq[0] = crho * p2 * (cte1 + cx10);
+    eq[1] = crho * p2 * (cte1 + cx11);
+    eq[2] = crho * p2 * (cte1 + cx12);
+    eq[3] = crho * p2 * (cte1 + cx13);
+    eq[4] = crho * p1 * (cte1 + cx14);
+}
+
+// Node of this thread under the warp-segment mapping of sweep_ab_kernel;
+// returns false for idle lanes.
+template <class S, class C, class IDX>
+__device__ __forceinline__ bool aa_node(const SweepArgs<S, C>& P, int& i, int& j, int& k, IDX& c) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t gw = blockIdx.x * 8u + (threadIdx.x >> 5);
+    const uint32_t row = P.div_seg.div(gw);
+    if (row >= P.nrows) return false;
+    const int seg = (int)(gw - row * (uint32_t)P.nseg);
+    const uint32_t kk = P.div_m.div(row);
+    j = (int)(row - kk * (uint32_t)P.m) + 1;
+    k = (int)kk + 1;
+    const IDX rowoff = (IDX)P.nx * (IDX)j + (IDX)P.nxy * (IDX)k;
+    const int sh = (int)((P.align_base + (long long)rowoff + 1) & 31);
+    i = seg * 32 + lane + 1 - (P.nseg_aligned ? 0 : sh);
+    if (i < 1 || i > P.l) return false;
+    c = rowoff + (IDX)i;
+    return true;
+}
+
+// Even (local) step.  P.a and P.b both name the slot arrays.
+template <class S, class C, int BC, class IDX, bool GENERIC>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(const SweepArgs<S, C> P) {
+    int i, j, k;
+    IDX c;
+    if (!aa_node<S, C, IDX>(P, i, j, k, c)) return;
+    if (P.obs != nullptr && i >= P.imin && i <= P.imax && j >= P.jmin && j <= P.jmax && k >= P.kmin &&
+        k <= P.kmax && (obstacle_links(P, i, j, k) & 0x80000000u))
+        return;
+    S** f = const_cast<S**>(P.a);
+    const float inv = P.inv_scale, scl = P.scale;
+    C x[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) x[d] = Conv<S, C>::ld(f[d][c], inv);
+    C y[19];
+    bgk_collide<C, GENERIC>(x, y, P.col);
+    S st[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) st[d] = Conv<S, C>::st(y[d], scl);
+#pragma unroll
+    for (int d = 0; d < 19; ++d) f[opp_of(d)][c] = st[d];
+    if (BC == BC_INFLOW && i == P.l) {
+        C s[19];
+#pragma unroll
+        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(st[d], inv);
+        C eq[5];
+        outflow_eq<C>(s, P.inflow_cte1, P.col, eq);
+#pragma unroll
+        for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::st(eq[e], scl);
+    }
+}
+
+// Odd (pull + push) step.
+template <class S, class C, int BC, class IDX, bool GENERIC>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(const SweepArgs<S, C> P) {
+    typedef Faces<BC> F;
+    int i, j, k;
+    IDX c;
+    if (!aa_node<S, C, IDX>(P, i, j, k, c)) return;
+    uint32_t sl = 0;
+    if (P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
+        j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1) {
+        sl = obstacle_links(P, i, j, k);
+        if (sl & 0x80000000u) return;
+    }
+    S** f = const_cast<S**>(P.a);
+    const IDX nx = (IDX)P.nx, nxy = (IDX)P.nxy;
+    // offset of the neighbour at -1 / +1 along each axis (periodic axes wrap)
+    const IDX oxm = (F::PX && i == 1) ? (IDX)(P.l - 1) : (IDX)(-1);
+    const IDX oxp = (F::PX && i == P.l) ? (IDX)(1 - P.l) : (IDX)1;
+    const IDX oym = (F::PY && j == 1) ? (IDX)(P.m - 1) * nx : -nx;
+    const IDX oyp = (F::PY && j == P.m) ? (IDX)(1 - P.m) * nx : nx;
+    const IDX ozm = (F::PZ && k == 1) ? (IDX)(P.n - 1) * nxy : -nxy;
+    const IDX ozp = (F::PZ && k == P.n) ? (IDX)(1 - P.n) * nxy : nxy;
+    // the -1 / +1 neighbour lies behind a wall
+    const bool wxm = F::WX && i == 1, wxp = F::WX && i == P.l;
+    const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
+    const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
+    const float inv = P.inv_scale, scl = P.scale;
+    C x[19];
+#pragma unroll
+    for (int d = 0; d < 18; ++d) {
+        const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+        // source x - c_d
+        IDX off = c;
+        if (cx == 1) off += oxm; else if (cx == -1) off += oxp;
+        if (cy == 1) off += oym; else if (cy == -1) off += oyp;
+        if (cz == 1) off += ozm; else if (cz == -1) off += ozp;
+        bool bounce = ((sl >> d) & 1u) != 0;
+        if (cx == 1) bounce |= wxm; else if (cx == -1) bounce |= wxp;
+        if (cy == 1) bounce |= wym; else if (cy == -1) bounce |= wyp;
+        if (cz == 1) bounce |= wzm; else if (cz == -1) bounce |= wzp;
+        C v = Conv<S, C>::ld(bounce ? f[d][c] : f[opp_of(d)][off], inv);
+        if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
+            v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force, scl, inv);
+        if (BC == BC_INFLOW && cx == 1 && i == 1)
+            v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col), scl, inv);
+        x[d] = v;
+    }
+    x[18] = Conv<S, C>::ld(f[18][c], inv);
+    C y[19];
+    bgk_collide<C, GENERIC>(x, y, P.col);
+#pragma unroll
+    for (int d = 0; d < 18; ++d) {
+        const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d), od = opp_of(d);
+        // target x + c_d
+        IDX off = c;
+        if (cx == 1) off += oxp; else if (cx == -1) off += oxm;
+        if (cy == 1) off += oyp; else if (cy == -1) off += oym;
+        if (cz == 1) off += ozp; else if (cz == -1) off += ozm;
+        bool bounce = ((sl >> od) & 1u) != 0;
+        if (cx == 1) bounce |= wxp; else if (cx == -1) bounce |= wxm;
+        if (cy == 1) bounce |= wyp; else if (cy == -1) bounce |= wym;
+        if (cz == 1) bounce |= wzp; else if (cz == -1) bounce |= wzm;
+        const S sv = Conv<S, C>::st(y[d], scl);
+        if (bounce) {
+            S bv = sv;
+            if (BC == BC_DRIVEN && (od == 1 || od == 10) && k == P.n) {
+                const C r = Conv<S, C>::ld(sv, inv);
+                bv = Conv<S, C>::st(od == 1 ? r + P.lid_force : r - P.lid_force, scl);
+            }
+            f[od][c] = bv;
+        } else {
+            const bool gone = BC == BC_INFLOW && ((cx == -1 && i == 1) || (cx == 1 && i == P.l));
+            if (!gone) f[d][off] = sv;
+        }
+    }
+    f[18][c] = Conv<S, C>::st(y[18], scl);
+    if (BC == BC_INFLOW && i == 1) {
+#pragma unroll
+        for (int d = 0; d < 5; ++d)
+            f[d][c] = Conv<S, C>::st(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col), scl);
+    }
+    if (BC == BC_INFLOW && i == P.l) {
+        C s[19];
+#pragma unroll
+        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(Conv<S, C>::st(y[d], scl), inv);
+        C eq[5];
+        outflow_eq<C>(s, P.inflow_cte1, P.col, eq);
+#pragma unroll
+        for (int e = 0; e < 5; ++e) {
+            const int d = 9 + e, cy = cy_of(d), cz = cz_of(d);
+            IDX off = c;   // (l+1, j, k) + c_d = (l, j + c_y, k + c_z)
+            if (cy == 1) off += oyp; else if (cy == -1) off += oym;
+            if (cz == 1) off += ozp; else if (cz == -1) off += ozm;
+            f[d][off] = Conv<S, C>::st(eq[e], scl);
+        }
+    }
+}
+
+// Outflow halo in slot form for a freshly loaded Layout E state: halo cell
+// (l+1, j, k) slot opp(p), p = 10..14, from the populations of (l, j, k).
+template <class S, class C>
+__global__ void aa_outflow_prepass_kernel(const SweepArgs<S, C> P) {
+    const int j = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int k = 1 + (int)blockIdx.y;
+    if (j > P.m) return;
+    S** f = const_cast<S**>(P.a);
+    const long long c = (long long)P.l + P.nx * (long long)j + P.nxy * (long long)k;
+    const float inv = P.inv_scale, scl = P.scale;
+    C s[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(f[opp_of(d)][c], inv);
+    C eq[5];
+    outflow_eq<C>(s, P.inflow_cte1, P.col, eq);
+#pragma unroll
+    for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::st(eq[e], scl);
+}
+
+}  // namespace bgk

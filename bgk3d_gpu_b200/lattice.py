@@ -129,3 +129,83 @@ class DeviceLattice:
                                  self._out.data_ptr(), ws.data_ptr(), ws.numel(), st),
               "bgk_draglift")
         return self._out[:3].cpu().numpy().copy()
+
+
+class Lattice:
+    """A library-owned lattice (bgk_lattice_*): padded aligned layout, AB or
+    in-place AA pattern, CUDA-graph replay of long step runs.  Host transfers
+    use the reference layout (19, n+2, m+2, l+2) in the storage representation."""
+
+    def __init__(self, l, m, n, kind="f32", bcase="periodic", omega=1.0, pattern="ab",
+                 lid_force=0.0, u_inflow=0.0, force_mode=0, force=(0.0, 0.0, 0.0), scale=1.0,
+                 device=None):
+        from ._lattice_abi import LatticeDesc
+        self.L = lib()
+        self.l, self.m, self.n = l, m, n
+        self.kind, self.bcase = _kind(kind), _bcase(bcase)
+        self.device = torch.device(device or "cuda")
+        d = LatticeDesc()
+        self.L.bgk_lattice_desc_init(ctypes.byref(d), self.kind, self.bcase, l, m, n, float(omega))
+        d.pattern = 1 if pattern in ("aa", 1) else 0
+        d.lid_force, d.u_inflow, d.force_mode = lid_force, u_inflow, force_mode
+        d.fx, d.fy, d.fz = force
+        d.scale = scale
+        self.desc = d
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(self.L.bgk_lattice_create(ctypes.byref(d), ctypes.byref(h)), "bgk_lattice_create")
+        self.h = h
+        self._out = torch.zeros(8, dtype=torch.float64, device=self.device)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bgk_lattice_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.L.bgk_lattice_device_bytes(ctypes.byref(self.desc)))
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def set_obstacle(self, obs: np.ndarray | None) -> None:
+        if obs is None:
+            check(self.L.bgk_lattice_set_obstacle(self.h, None), "set_obstacle")
+            return
+        o = np.ascontiguousarray(obs, np.int32)
+        check(self.L.bgk_lattice_set_obstacle(self.h, o.ctypes.data), "set_obstacle")
+
+    def upload(self, state: np.ndarray) -> None:
+        st = np.ascontiguousarray(state)
+        check(self.L.bgk_lattice_load(self.h, st.ctypes.data, self._stream()), "bgk_lattice_load")
+        torch.cuda.current_stream(self.device).synchronize()
+
+    def download(self) -> np.ndarray:
+        dt = {0: np.float64, 1: np.float32, 2: np.uint16, 3: np.uint16, 4: np.float32}[self.kind]
+        out = np.empty((19, self.n + 2, self.m + 2, self.l + 2), dt)
+        check(self.L.bgk_lattice_store(self.h, out.ctypes.data, self._stream()), "bgk_lattice_store")
+        torch.cuda.current_stream(self.device).synchronize()
+        return out
+
+    def step(self, nsteps=1) -> None:
+        check(self.L.bgk_lattice_step(self.h, int(nsteps), self._stream()), "bgk_lattice_step")
+
+    @property
+    def steps(self) -> int:
+        return int(self.L.bgk_lattice_steps(self.h))
+
+    def moments(self) -> np.ndarray:
+        check(self.L.bgk_lattice_moments(self.h, self._out.data_ptr(), self._stream()), "moments")
+        return self._out[:5].cpu().numpy().copy()
+
+    def draglift(self, box) -> np.ndarray:
+        check(self.L.bgk_lattice_draglift(self.h, *[int(v) for v in box], self._out.data_ptr(),
+                                          self._stream()), "draglift")
+        return self._out[:3].cpu().numpy().copy()

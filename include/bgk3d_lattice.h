@@ -1,0 +1,90 @@
+/*
+ * bgk3d_lattice.h -- library-owned lattices (part of libbgk3d_b200.so).
+ *
+ * A bgk_lattice holds its populations in device memory in a padded layout
+ * (row pitch a multiple of 32 elements, node (1,j,k) on a 128-byte boundary)
+ * and advances them with the fused sweep, either as two lattices (AB, the
+ * reference's ping-pong, SRC/col_MC.F90:539-596) or in place (AA: one
+ * population set, half the memory).  Host transfers use the reference's own
+ * layout: 19 consecutive arrays (0:l+1, 0:m+1, 0:n+1), i fastest, in the
+ * storage kind's representation (raw 16-bit words for the 16-bit kinds),
+ * which is the record layout of SRC/restore_raw.F90:43-61 without markers.
+ *
+ * Reference counterparts: the Fortran driver's allocation and time loop
+ * (SRC/alloca.F90:150-191, SRC/bgk3d.F90:169-196) for one case.
+ */
+#ifndef BGK3D_LATTICE_H
+#define BGK3D_LATTICE_H
+
+#include "bgk3d_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BGK_PATTERN_AB 0   /* two population sets, pointer swap (reference scheme) */
+#define BGK_PATTERN_AA 1   /* one population set, in place                        */
+
+typedef struct bgk_lattice bgk_lattice;
+
+typedef struct bgk_lattice_desc {
+    int kind;              /* BGK_KIND_* */
+    int bcase;             /* BGK_BC_DRIVEN / PERIODIC / CHANNEL / INFLOW */
+    int pattern;           /* BGK_PATTERN_AB or BGK_PATTERN_AA */
+    int l, m, n;           /* interior extents */
+    double omega;          /* BGK relaxation frequency */
+    int force_mode;        /* 0: constant per-population force; 1: force * rho */
+    double fx, fy, fz;
+    double lid_force;      /* DRIVEN: u_lid / 6 */
+    double u_inflow;       /* INFLOW */
+    float scale;           /* 16-bit kinds: power-of-two storage scale */
+} bgk_lattice_desc;
+
+/* Defaults: AB pattern, no force, lid 0, inflow 0, scale 1. */
+void bgk_lattice_desc_init(bgk_lattice_desc* d, int kind, int bcase, int l, int m, int n, double omega);
+
+/* Device bytes a lattice with this description occupies (admission control). */
+size_t bgk_lattice_device_bytes(const bgk_lattice_desc* d);
+
+/* Allocate the lattice on the current device (cudaMalloc). */
+int bgk_lattice_create(const bgk_lattice_desc* d, bgk_lattice** out);
+int bgk_lattice_destroy(bgk_lattice* lat);
+
+/* Obstacle mask obs_host[l*m*n] (i fastest, 1 = solid, SRC/build.obs.F90
+   convention); copied to the device, bounding box computed here.  Must stay
+   one node inside the lattice.  NULL removes the obstacle. */
+int bgk_lattice_set_obstacle(bgk_lattice* lat, const int32_t* obs_host);
+
+/* Load / store the post-collision state in the reference layout (see top).
+   Stream-ordered; host memory should be pinned for asynchrony.  store needs
+   an even number of AA steps since the last load (BGK_ERR_STATE otherwise). */
+int bgk_lattice_load(bgk_lattice* lat, const void* host, void* stream);
+int bgk_lattice_store(const bgk_lattice* lat, void* host, void* stream);
+
+/* Advance nsteps time steps (boundaries + stream + collide), stream-ordered.
+   Runs of 16 or more steps replay a captured CUDA graph. */
+int bgk_lattice_step(bgk_lattice* lat, int nsteps, void* stream);
+
+/* Change the relaxation frequency / force of an existing lattice. */
+int bgk_lattice_set_omega(bgk_lattice* lat, double omega);
+
+/* FP64 moments (as bgk_moments) of the current state into out_dev[0..4];
+   AA lattices need an even step count. */
+int bgk_lattice_moments(const bgk_lattice* lat, double* out_dev, void* stream);
+
+/* FP64 drag/lift (as bgk_draglift) over the box into out_dev[0..2]. */
+int bgk_lattice_draglift(const bgk_lattice* lat, int is, int ie, int js, int je, int ks, int ke,
+                         double* out_dev, void* stream);
+
+/* Steps advanced since the last load. */
+long long bgk_lattice_steps(const bgk_lattice* lat);
+
+/* Current population pointers (device) and the layout, for callers that
+   run their own kernels on the state: a[19] in reference population order
+   (AA: valid after an even step count), nx/ny leading dimensions. */
+int bgk_lattice_arrays(const bgk_lattice* lat, void** a19, long long* nx, long long* ny);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BGK3D_LATTICE_H */
