@@ -123,16 +123,6 @@ def _dist():
     return ws, rank, local
 
 
-def _max_over_ranks(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
 def _barrier(ws: int):
     if ws > 1:
         import torch.distributed as dist
@@ -297,9 +287,11 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = e0.elapsed_time(e1)
-    ms_max = _max_over_ranks(ms, ws)
     nodes = L_ * M_ * N_
-    value = nodes * args.steps * ws / (ms_max * 1e-3) / 1e9
+    from bgk3d_gpu_b200.replicas import job_throughput
+    _, t_max, rate = job_throughput(float(nodes) * args.steps, ms * 1e-3)
+    ms_max = t_max * 1e3
+    value = rate / 1e9
     launch_s = ms * 1e-3 / args.steps
     achieved = B_ALG_F32 * nodes / launch_s / 1e9
     peak, peak_src = _peaks()

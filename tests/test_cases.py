@@ -1,0 +1,54 @@
+"""CPU checks of the case builders: the reference's obstacle builder
+(SRC/build.obs.F90:52-97) restated loop by loop, the solid sphere of the
+flow-past-a-sphere configuration, and the collision parameters."""
+import numpy as np
+
+from bgk3d_gpu_b200 import cases as CS
+
+
+def _build_obs_loops(l, m, n, ly):
+    """Literal loop restatement of SRC/build.obs.F90:52-97."""
+    imin, jmin, kmin, imax, jmax, kmax = l, m, n, 0, 0, 0
+    ic, jc, kc = 2 * l // 5, m // 2, n // 2
+    radius = 32 if m > 256 else ly // 8
+    R = radius * 1.0
+    r2a, r2b = (R - 2) * (R - 2), (R + 2) * (R + 2)
+    obs = np.zeros((n, m, l), np.int32)
+    for k in range(1, n + 1):
+        for j in range(1, m + 1):
+            for i in range(1, l + 1):
+                d2 = float((ic - i) * (ic - i) + (jc - j) * (jc - j) + (kc - k) * (kc - k))
+                if d2 > r2a and d2 < r2b:
+                    obs[k - 1, j - 1, i - 1] = 1
+                    imin, jmin, kmin = min(imin, i), min(jmin, j), min(kmin, k)
+                    imax, jmax, kmax = max(imax, i), max(jmax, j), max(kmax, k)
+    return obs, radius, (imin, imax, jmin, jmax, kmin, kmax)
+
+
+def test_reference_shell_matches_loop_restatement():
+    for (l, m, n) in [(64, 48, 40), (50, 32, 32)]:
+        obs, radius, bbox = CS.reference_shell_obstacle(l, m, n)
+        o2, r2, b2 = _build_obs_loops(l, m, n, m)
+        assert radius == r2 and bbox == b2
+        assert np.array_equal(obs, o2)
+
+
+def test_solid_sphere_of_benchmark_config():
+    case = CS.sphere()
+    obs = case["obstacle"]
+    assert obs.shape == (256, 256, 512)
+    # D = 40 centred at (128,128,128): 4/3 pi 20^3 ~ 33510 nodes
+    assert abs(int(obs.sum()) - 4.0 / 3.0 * np.pi * 20 ** 3) < 600
+    assert case["drag_box"] == (105, 151, 105, 151, 105, 151)
+    assert abs(1.0 / case["omega"] - (3 * 0.05 * 40 / 300 + 0.5)) < 1e-15
+
+
+def test_collision_parameters():
+    ldc = CS.lid_driven_cavity()
+    assert abs(ldc["nu"] - 0.032) < 1e-15 and abs(1 / ldc["omega"] - 0.596) < 1e-12
+    assert abs(ldc["lid_force"] - 0.1 / 6) < 1e-17
+    tgv = CS.taylor_green()
+    assert abs(1 / tgv["omega"] - 0.524) < 1e-12
+    assert abs(CS.omega_from_nu(0.032) - 1 / 0.596) < 1e-12
+    pof = CS.poiseuille(32, 0.6)
+    assert pof["force_mode"] == 1 and pof["force"][0] == 1e-7
