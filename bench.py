@@ -53,7 +53,7 @@ def _traffic_from_profile():
     try:
         for line in open(path):
             if line.strip().startswith("dram_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].strip().split()[0])
+                return float(line.split(":", 1)[1].strip().split()[0]) * 1e6   # MB -> bytes
     except OSError:
         pass
     return None
@@ -333,7 +333,8 @@ def run_ours(args):
                    "parallelism": f"replicas x{ws}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
-                     "traffic": traffic, "b_alg_per_lup": B_ALG_F32,
+                     "traffic": traffic, "traffic_unit": "bytes per launch (ncu, profiles/sweep_ab_f32_tgv256.md)",
+                     "algorithmic_bytes_per_launch": B_ALG_F32 * nodes, "b_alg_per_lup": B_ALG_F32,
                      "kernel": "sweep_ab_kernel<float,float,PERIODIC,int,false>" if args.pattern == "ab"
                      else "aa_odd_kernel + aa_even_kernel <float,float,PERIODIC,int,false>"},
         "cpu_baseline": {"value": cpu[0], "unit": "GLUPS", "cores": cpu[1], "kind": "port",
