@@ -350,42 +350,44 @@ def run_ours(args):
 
 
 def run_e2e(host, args):
-    """Same workload through the reference's C ABI (bcond_periodic_gpu + col_mc_gpu
-    of libbgk3d_dropin_sp.so), from pinned host memory: H2D of the initial
-    state, every step the FP64 kinetic-energy reduction read back to the host,
-    D2H of the final state."""
+    """Same workload through the reference's C ABI (bcond_periodic_gpu +
+    col_mc_gpu of libbgk3d_dropin_sp.so, the reference's Fortran array
+    layout), from pinned host memory: H2D of the initial state, every step the
+    FP64 kinetic-energy sums (computed in the same pass as the step) copied to
+    pinned host memory, D2H of the final state; one synchronisation at the end."""
     import torch
     from bgk3d_gpu_b200 import _lib
     D = _lib.load_dropin(False)
-    L = _lib.lib()
+    steps = args.e2e_steps
     host_out = torch.empty_like(host).pin_memory()
-    ke_host = torch.empty(5, dtype=torch.float64).pin_memory()
-    A = torch.empty(host.shape, dtype=host.dtype, device="cuda")
-    B = torch.empty((18,) + tuple(host.shape[1:]), dtype=host.dtype, device="cuda")
-    a = [A[d] for d in range(19)]
-    b = [B[d] for d in range(18)]
+    ke_host = torch.empty((steps + 8, 5), dtype=torch.float64).pin_memory()
+    # one device array per population, as the Fortran driver allocates them
+    a = [torch.empty(host.shape[1:], dtype=host.dtype, device="cuda") for _ in range(19)]
+    b = [torch.empty(host.shape[1:], dtype=host.dtype, device="cuda") for _ in range(18)]
+    a0, b0 = list(a), list(b)
     nx, ny = L_ + 2, M_ + 2
-    ws_bytes = L.bgk_reduce_workspace_bytes(L_, M_, N_)
-    wsp = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
-    out = torch.empty(5, dtype=torch.float64, device="cuda")
-    p = _lib.sweep_params(_lib.KIND_F32, L_, M_, N_, OMEGA)
+    out = torch.empty((steps + 8, 5), dtype=torch.float64, device="cuda")
     stream = torch.cuda.default_stream()
-    steps = max(10, args.steps // 4)
+    D.bgk_dropin_reset()
+    D.bgk_dropin_track_moments(1)
 
     def one_run(nsteps):
-        A.copy_(host, non_blocking=True)
-        for _ in range(nsteps):
+        a[:] = a0
+        b[:] = b0
+        for d in range(19):
+            a[d].copy_(host[d], non_blocking=True)
+        for s in range(nsteps):
             pa = (ctypes.c_void_p * 19)(*[t.data_ptr() for t in a])
             D.bcond_periodic_gpu(pa, L_, M_, N_, nx, ny)
             D.col_mc_gpu(*[t.data_ptr() for t in a], *[t.data_ptr() for t in b], L_, M_, N_, nx, ny,
                          OMEGA, 0.0, 1.0, 1 / 3, 1 / 18, 1 / 36, 3.0, 1.5, 3.0, 0.0, 0.0, 0.0)
             for d in range(18):
                 a[d], b[d] = b[d], a[d]
-            _lib.check(L.bgk_moments(ctypes.byref(p), _lib.ptr_array([t.data_ptr() for t in a]),
-                                     out.data_ptr(), wsp.data_ptr(), ws_bytes, None), "bgk_moments")
-            ke_host.copy_(out, non_blocking=True)
-            stream.synchronize()
-        host_out.copy_(torch.stack(a), non_blocking=True)
+            if D.bgk_dropin_moments(out[s].data_ptr(), None) != 0:
+                raise RuntimeError("bgk_dropin_moments failed")
+            ke_host[s].copy_(out[s], non_blocking=True)
+        for d in range(19):
+            host_out[d].copy_(a[d], non_blocking=True)
         stream.synchronize()
 
     with torch.cuda.stream(stream):
@@ -394,12 +396,16 @@ def run_e2e(host, args):
         t0 = time.perf_counter()
         one_run(steps)
         dt = time.perf_counter() - t0
+    D.bgk_dropin_track_moments(0)
+    D.bgk_dropin_reset()
     state_bytes = host.numel() * host.element_size()
     return {"value": L_ * M_ * N_ * steps / dt / 1e9, "unit": "GLUPS",
             "h2d_bytes_per_step": state_bytes / steps,
             "d2h_bytes_per_step": state_bytes / steps + 40,
             "steps": steps,
-            "path": "drop-in C ABI (bcond_periodic_gpu + col_mc_gpu) + per-step FP64 KE to host"}
+            "ke_mean_last": float(ke_host[steps - 1, 4]) / (L_ * M_ * N_),
+            "path": "drop-in C ABI (bcond_periodic_gpu + col_mc_gpu, reference layout) with the per-step FP64 "
+                    "kinetic energy fused into the step and copied to the host every step"}
 
 
 def main():
@@ -410,6 +416,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--lattice", type=int, nargs=3, default=None, metavar=("L", "M", "N"),
                     help="override the lattice extents (profiling runs of a smaller case)")
+    ap.add_argument("--e2e-steps", type=int, default=2000,
+                    help="steps of the end-to-end solve (the TGV configuration runs 2000)")
     ap.add_argument("--pattern", default="ab", choices=["ab", "aa"],
                     help="two-lattice (ab) or in-place (aa) streaming")
     ap.add_argument("--kernel-only", action="store_true",

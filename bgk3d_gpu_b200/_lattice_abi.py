@@ -34,6 +34,8 @@ def bind(L) -> None:
     L.bgk_lattice_store.restype = c_int
     L.bgk_lattice_step.argtypes = [c_void_p, c_int, c_void_p]
     L.bgk_lattice_step.restype = c_int
+    L.bgk_lattice_step_moments.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p]
+    L.bgk_lattice_step_moments.restype = c_int
     L.bgk_lattice_set_omega.argtypes = [c_void_p, c_double]
     L.bgk_lattice_set_omega.restype = c_int
     L.bgk_lattice_moments.argtypes = [c_void_p, c_void_p, c_void_p]

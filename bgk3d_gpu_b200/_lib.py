@@ -76,6 +76,11 @@ def lib() -> ctypes.CDLL:
     L.bgk_moments_noalloc.restype = c_int
     L.bgk_moments_noalloc_max_bytes.argtypes = []
     L.bgk_moments_noalloc_max_bytes.restype = c_size_t
+    L.bgk_sweep_moments_workspace_bytes.argtypes = [P]
+    L.bgk_sweep_moments_workspace_bytes.restype = c_size_t
+    L.bgk_sweep_moments.argtypes = [P, POINTER(c_void_p), POINTER(c_void_p), c_void_p, c_void_p, c_size_t,
+                                    c_void_p]
+    L.bgk_sweep_moments.restype = c_int
     L.bgk_draglift.argtypes = [P, POINTER(c_void_p), c_int, c_int, c_int, c_int, c_int, c_int,
                                c_void_p, c_void_p, c_size_t, c_void_p]
     L.bgk_draglift.restype = c_int
@@ -138,7 +143,11 @@ def load_dropin(double: bool) -> ctypes.CDLL:
     D.bcond_inflow_gpu.argtypes = [pa, c_int, c_int, c_int, c_int, c_int] + [real] * 7
     D.bcond_obs_gpu.argtypes = [pa, c_void_p] + [c_int] * 13
     D.gpu_device_sync.argtypes = []
+    D.bgk_dropin_track_moments.argtypes = [c_int]
+    D.bgk_dropin_track_moments.restype = None
+    D.bgk_dropin_moments.argtypes = [c_void_p, c_void_p]
+    D.bgk_dropin_moments.restype = c_int
     for f in ("bcond_periodic_gpu", "bcond_channel_gpu", "bcond_driven_gpu", "bcond_inflow_gpu",
-              "bcond_obs_gpu", "gpu_device_sync", "bgk_dropin_reset"):
+              "bcond_obs_gpu", "gpu_device_sync", "bgk_dropin_reset", "bgk_dropin_track_moments"):
         getattr(D, f).restype = None
     return D

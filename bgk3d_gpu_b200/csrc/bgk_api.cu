@@ -7,9 +7,8 @@
 #include <string>
 #include "bgk3d_b200.h"
 #include "bgk_internal.h"
-#include "sweep_ab.cuh"
+#include "kernels.h"
 #include "reduce.cuh"
-#include "host_args.cuh"
 
 namespace bgk {
 
@@ -35,6 +34,30 @@ dim3 row_block(int l) {
     int tx = 32;
     while (tx < l && tx < 256) tx <<= 1;
     return dim3(tx, 256 / tx, 1);
+}
+
+void moments_grid(int l, int m, int n, dim3& grd, dim3& blk) {
+    blk = row_block(l);
+    int kb = n < 64 ? n : 64;
+    grd = dim3((l + blk.x - 1) / blk.x, (m + blk.y - 1) / blk.y, kb);
+}
+
+long long sweep_blocks(const bgk_sweep_params* p, const void* a0) {
+    // the warp-segment launch of sweep_ab_kernel / the AA kernels: rows that
+    // start on a 32-element boundary need ceil(l/32) segments, others one more
+    const size_t es = p->kind == 0 ? 8 : (p->kind == 2 || p->kind == 3) ? 2 : 4;
+    bool aligned = false;
+    if (a0) {
+        const long long elem = (long long)((uintptr_t)a0 / es);
+        aligned = (((elem & 31) + 1) % 32 == 0) && (p->nx % 32 == 0);
+    }
+    const long long nseg = aligned ? (p->l + 31) / 32 : (p->l + 62) / 32;
+    return (nseg * p->m * p->n + 7) / 8;
+}
+
+int finalize_moments(const double* partials, long long nparts, double* out, cudaStream_t st) {
+    finalize_partials_kernel<5><<<1, 256, 0, st>>>(partials, nparts, out);
+    return check_launch("finalize_partials_kernel");
 }
 
 int validate(const bgk_sweep_params* p) {
@@ -65,97 +88,21 @@ int validate(const bgk_sweep_params* p) {
     return BGK_OK;
 }
 
-template <class S, class C, int BC>
-void launch_sweep_bc(const SweepArgs<S, C>& A, long long nelem, unsigned blocks, bool generic,
-                     cudaStream_t st) {
-    if (nelem < (1LL << 31)) {
-        if (generic) sweep_ab_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
-        else sweep_ab_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
-    } else {
-        if (generic) sweep_ab_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
-        else sweep_ab_kernel<S, C, BC, long long, false><<<blocks, 256, 0, st>>>(A);
-    }
-}
-
-template <class S, class C>
-int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, cudaStream_t st) {
-    SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
-    segment_geometry(A, a[0]);
-    if (p->bcase == BC_INFLOW) {
-        dim3 blk(128), grd((p->m + 127) / 128, p->n);
-        outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
-        if (int e = check_launch("outflow_halo_kernel")) return e;
-    }
-    const long long warps = (long long)A.nseg * p->m * p->n;
-    const long long blocks = (warps + 7) / 8;
-    if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
-    const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
-    const bool g = generic_collision(p);
-    const unsigned nb = (unsigned)blocks;
-    switch (p->bcase) {
-        case BC_NONE: launch_sweep_bc<S, C, BC_NONE>(A, nelem, nb, g, st); break;
-        case BC_DRIVEN: launch_sweep_bc<S, C, BC_DRIVEN>(A, nelem, nb, g, st); break;
-        case BC_PERIODIC: launch_sweep_bc<S, C, BC_PERIODIC>(A, nelem, nb, g, st); break;
-        case BC_CHANNEL: launch_sweep_bc<S, C, BC_CHANNEL>(A, nelem, nb, g, st); break;
-        case BC_INFLOW: launch_sweep_bc<S, C, BC_INFLOW>(A, nelem, nb, g, st); break;
-    }
-    return check_launch("sweep_ab_kernel");
-}
-
-// Grid of the moments pass: rows of the (i, j) plane x KB blocks striding k.
-void moments_grid(int l, int m, int n, dim3& grd, dim3& blk) {
-    blk = row_block(l);
-    int kb = n < 64 ? n : 64;
-    grd = dim3((l + blk.x - 1) / blk.x, (m + blk.y - 1) / blk.y, kb);
-}
-
-template <class S, class C>
-int launch_moments(const bgk_sweep_params* p, void* const* a, double* out, double* ws, cudaStream_t st) {
-    FieldArgs<S, C> F = field_args<S, C>(p, a);
-    dim3 grd, blk;
-    moments_grid(p->l, p->m, p->n, grd, blk);
-    moments_partial_kernel<S, C><<<grd, blk, 0, st>>>(F, ws);
-    if (int e = check_launch("moments_partial_kernel")) return e;
-    const long long nparts = (long long)grd.x * grd.y * grd.z;
-    finalize_partials_kernel<5><<<1, 256, 0, st>>>(ws, nparts, out);
-    return check_launch("finalize_partials_kernel");
-}
-
-template <class S, class C>
-int launch_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks, int ke,
-                    double* out, double* ws, size_t ws_bytes, cudaStream_t st) {
-    FieldArgs<S, C> F = field_args<S, C>(p, a);
-    const int ni = ie - is + 1, nj = je - js + 1, nk = ke - ks + 1;
-    const long long tot = (long long)ni * nj * nk;
-    const long long nb = (tot + 255) / 256;
-    if ((size_t)nb * 3 * sizeof(double) > ws_bytes)
-        return set_error(BGK_ERR_ARG, "draglift box needs %lld bytes of workspace", nb * 3 * 8);
-    draglift_partial_kernel<S, C><<<(unsigned)nb, 256, 0, st>>>(F, is, js, ks, ni, nj, nk, ws);
-    if (int e = check_launch("draglift_partial_kernel")) return e;
-    finalize_partials_kernel<3><<<1, 256, 0, st>>>(ws, nb, out);
-    return check_launch("finalize_partials_kernel");
-}
-
 }  // namespace bgk
 
 using namespace bgk;
-
-#define KIND_DISPATCH(kind, CALL)                                                     \
-    switch (kind) {                                                                   \
-        case K_F64: { typedef double S; typedef double C; return CALL; }              \
-        case K_F32: { typedef float S; typedef float C; return CALL; }                \
-        case K_F16: { typedef __half S; typedef float C; return CALL; }               \
-        case K_BF16: { typedef __nv_bfloat16 S; typedef float C; return CALL; }       \
-        case K_F32_F64: { typedef float S; typedef double C; return CALL; }           \
-    }                                                                                 \
-    return set_error(BGK_ERR_ARG, "bad kind");
 
 int bgk::moments_launch(const bgk_sweep_params* p, void* const* a, double* out, double* ws, cudaStream_t st) {
     KIND_DISPATCH(p->kind, (launch_moments<S, C>(p, a, out, ws, st)));
 }
 
 int bgk::sweep_launch(const bgk_sweep_params* p, void* const* a, void* const* b, cudaStream_t st) {
-    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, st)));
+    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, nullptr, st)));
+}
+
+int bgk::sweep_launch_mom(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom,
+                          cudaStream_t st) {
+    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, mom, st)));
 }
 
 int bgk::draglift_launch(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
@@ -185,6 +132,25 @@ int bgk_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, void* s
     for (int d = 0; d < 19; ++d)
         if (!a[d] || (d < 18 && !b[d])) return set_error(BGK_ERR_ARG, "null population %d", d + 1);
     return bgk::sweep_launch(p, a, b, (cudaStream_t)stream);
+}
+
+size_t bgk_sweep_moments_workspace_bytes(const bgk_sweep_params* p) {
+    if (!p) return 0;
+    return (size_t)bgk::sweep_blocks(p, nullptr) * 5 * sizeof(double);
+}
+
+int bgk_sweep_moments(const bgk_sweep_params* p, void* const* a, void* const* b, double* out_dev, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+    if (int e = validate(p)) return e;
+    if (!a || !b || !out_dev || !workspace) return set_error(BGK_ERR_ARG, "null pointer");
+    for (int d = 0; d < 19; ++d)
+        if (!a[d] || (d < 18 && !b[d])) return set_error(BGK_ERR_ARG, "null population %d", d + 1);
+    const long long nb = bgk::sweep_blocks(p, a[0]);
+    if (workspace_bytes < (size_t)nb * 5 * sizeof(double))
+        return set_error(BGK_ERR_ARG, "workspace too small: %zu < %zu", workspace_bytes, (size_t)nb * 40);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (int rc = bgk::sweep_launch_mom(p, a, b, (double*)workspace, st)) return rc;
+    return bgk::finalize_moments((const double*)workspace, nb, out_dev, st);
 }
 
 size_t bgk_reduce_workspace_bytes(int l, int m, int n) {
@@ -217,6 +183,22 @@ int bgk_device_sync(void) {
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "device sync failed: %s", cudaGetErrorString(e));
     return BGK_OK;
+}
+
+int bgk_dropin_sweep_tracked(const bgk_sweep_params* p, void* const* a, void* const* b, double* partials,
+                             size_t bytes, long long* nparts) {
+    if (int e = validate(p)) return e;
+    const long long nb = bgk::sweep_blocks(p, a[0]);
+    if (!partials || bytes < (size_t)nb * 5 * sizeof(double)) {
+        *nparts = 0;
+        return bgk::sweep_launch(p, a, b, nullptr);
+    }
+    *nparts = nb;
+    return bgk::sweep_launch_mom(p, a, b, partials, nullptr);
+}
+
+int bgk_dropin_finalize(const double* partials, long long nparts, double* out_dev, void* stream) {
+    return bgk::finalize_moments(partials, nparts, out_dev, (cudaStream_t)stream);
 }
 
 const char* bgk_last_error(void) { return g_last_error.c_str(); }

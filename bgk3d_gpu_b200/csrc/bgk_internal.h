@@ -11,6 +11,8 @@ int set_error(int code, const char* fmt, ...);
 int check_launch(const char* what);
 // Block shape for one-thread-per-node sweeps over (i, j) rows: TX x TY = 256.
 dim3 row_block(int l);
+// Grid of the moments pass: rows of the (i, j) plane x KB blocks striding k.
+void moments_grid(int l, int m, int n, dim3& grd, dim3& blk);
 // Parameter checks shared by every entry point (returns BGK_OK or an error).
 int validate(const struct bgk_sweep_params* p);
 // The two launches of the FP64 moments reduction, with the per-block
@@ -19,6 +21,14 @@ int moments_launch(const struct bgk_sweep_params* p, void* const* a, double* out
                    cudaStream_t st);
 // The fused sweep launch(es) without argument validation.
 int sweep_launch(const struct bgk_sweep_params* p, void* const* a, void* const* b, cudaStream_t st);
+// Same, with the per-block FP64 moments of the new state written to mom.
+int sweep_launch_mom(const struct bgk_sweep_params* p, void* const* a, void* const* b, double* mom,
+                     cudaStream_t st);
+// Number of blocks (= partial-moment slots) of the sweep launch for p with
+// population 01 at a0 (nullptr: the upper bound for any alignment).
+long long sweep_blocks(const struct bgk_sweep_params* p, const void* a0);
+// Second pass over nparts partials of 5 doubles into out[0..4].
+int finalize_moments(const double* partials, long long nparts, double* out, cudaStream_t st);
 // The two launches of the FP64 drag/lift reduction.
 int draglift_launch(const struct bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
                     int ke, double* out, double* ws, size_t ws_bytes, cudaStream_t st);

@@ -23,6 +23,15 @@ struct Pending {
 };
 thread_local Pending g_pending;
 
+// Optional FP64 moments of the state each col_mc_gpu writes (same pass).
+struct Tracked {
+    bool on = false;
+    double* partials = nullptr;
+    size_t bytes = 0;
+    long long nparts = 0;
+};
+thread_local Tracked g_tracked;
+
 #if defined(DOUBLE_P) || defined(GPU_DOUBLE)
 constexpr int kKind = BGK_KIND_F64;
 #else
@@ -125,7 +134,19 @@ void col_mc_gpu(const real_t* a01, const real_t* a02, const real_t* a03, const r
     }
     g.bcase = BGK_BC_NONE;
     g.has_obs = false;
-    const int rc = bgk_sweep(&p, a, b, nullptr);
+    int rc;
+    Tracked& t = g_tracked;
+    if (t.on) {
+        const size_t need = bgk_sweep_moments_workspace_bytes(&p);
+        if (t.bytes < need) {
+            if (t.partials) cudaFree(t.partials);
+            t.partials = nullptr; t.bytes = 0;
+            if (cudaMalloc(&t.partials, need) == cudaSuccess) t.bytes = need;
+        }
+        rc = bgk_dropin_sweep_tracked(&p, a, b, t.partials, t.bytes, &t.nparts);
+    } else {
+        rc = bgk_sweep(&p, a, b, nullptr);
+    }
     if (rc != BGK_OK) {
         fprintf(stderr, "ERROR: col_mc_gpu: %s\n", bgk_last_error());
         fflush(stderr);
@@ -141,6 +162,17 @@ void gpu_device_sync(void) {
     }
 }
 
-void bgk_dropin_reset(void) { g_pending = Pending(); }
+void bgk_dropin_reset(void) {
+    g_pending = Pending();
+    if (g_tracked.partials) cudaFree(g_tracked.partials);
+    g_tracked = Tracked();
+}
+
+void bgk_dropin_track_moments(int on) { g_tracked.on = (on != 0); }
+
+int bgk_dropin_moments(double* out_dev, void* stream) {
+    if (!g_tracked.on || g_tracked.nparts <= 0 || !g_tracked.partials) return BGK_ERR_STATE;
+    return bgk_dropin_finalize(g_tracked.partials, g_tracked.nparts, out_dev, stream);
+}
 
 }  // extern "C"

@@ -9,8 +9,8 @@
 #include "bgk3d_b200.h"
 #include "bgk3d_lattice.h"
 #include "bgk_internal.h"
-#include "host_args.cuh"
-#include "sweep_aa.cuh"
+#include "kernels.h"
+#include "d3q19.cuh"
 
 using namespace bgk;
 
@@ -31,6 +31,8 @@ struct bgk_lattice {
     cudaStream_t cap_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    double* mom = nullptr;       // per-block partial moments of fused steps
+    size_t mom_bytes = 0;
 };
 
 namespace {
@@ -67,67 +69,12 @@ void drop_graph(bgk_lattice* L) {
     L->graph_steps = 0;
 }
 
-template <class S, class C, int BC>
-void launch_aa_bc(const SweepArgs<S, C>& A, bool odd, bool generic, long long nelem, unsigned blocks,
-                  cudaStream_t st) {
-    if (nelem < (1LL << 31)) {
-        if (odd) {
-            if (generic) aa_odd_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
-            else aa_odd_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
-        } else {
-            if (generic) aa_even_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
-            else aa_even_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
-        }
-    } else {
-        if (odd) aa_odd_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
-        else aa_even_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
-    }
-}
-
-template <class S, class C>
-int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, cudaStream_t st) {
-    SweepArgs<S, C> A = sweep_args<S, C>(p, slots, slots);
-    A.b[18] = (S*)slots[18];
-    segment_geometry(A, slots[0]);
-    const long long warps = (long long)A.nseg * p->m * p->n;
-    if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
-    const unsigned blocks = (unsigned)((warps + 7) / 8);
-    const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
-    const bool g = generic_collision(p);
-    switch (p->bcase) {
-        case BC_DRIVEN: launch_aa_bc<S, C, BC_DRIVEN>(A, odd, g, nelem, blocks, st); break;
-        case BC_PERIODIC: launch_aa_bc<S, C, BC_PERIODIC>(A, odd, g, nelem, blocks, st); break;
-        case BC_CHANNEL: launch_aa_bc<S, C, BC_CHANNEL>(A, odd, g, nelem, blocks, st); break;
-        case BC_INFLOW: launch_aa_bc<S, C, BC_INFLOW>(A, odd, g, nelem, blocks, st); break;
-        default: return set_error(BGK_ERR_ARG, "AA lattices need a boundary case");
-    }
-    return check_launch(odd ? "aa_odd_kernel" : "aa_even_kernel");
-}
-
-template <class S, class C>
-int launch_aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
-    SweepArgs<S, C> A = sweep_args<S, C>(p, slots, slots);
-    dim3 blk(128), grd((p->m + 127) / 128, p->n);
-    aa_outflow_prepass_kernel<S, C><<<grd, blk, 0, st>>>(A);
-    return check_launch("aa_outflow_prepass_kernel");
-}
-
-#define LKIND_DISPATCH(kind, CALL)                                                  \
-    switch (kind) {                                                                 \
-        case K_F64: { typedef double S; typedef double C; return CALL; }            \
-        case K_F32: { typedef float S; typedef float C; return CALL; }              \
-        case K_F16: { typedef __half S; typedef float C; return CALL; }             \
-        case K_BF16: { typedef __nv_bfloat16 S; typedef float C; return CALL; }     \
-        case K_F32_F64: { typedef float S; typedef double C; return CALL; }         \
-    }                                                                               \
-    return set_error(BGK_ERR_ARG, "bad kind");
-
-int aa_step(const bgk_sweep_params* p, void* const* slots, bool odd, cudaStream_t st) {
-    LKIND_DISPATCH(p->kind, (launch_aa<S, C>(p, slots, odd, st)));
+int aa_step(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st) {
+    KIND_DISPATCH(p->kind, (launch_aa<S, C>(p, slots, odd, mom, st)));
 }
 
 int aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
-    LKIND_DISPATCH(p->kind, (launch_aa_prepass<S, C>(p, slots, st)));
+    KIND_DISPATCH(p->kind, (launch_aa_prepass<S, C>(p, slots, st)));
 }
 
 // AA: population p of the observable state lives in slot opp(p).
@@ -138,13 +85,14 @@ void observable(const bgk_lattice* L, void** out) {
         for (int d = 0; d < 19; ++d) out[d] = L->a[d];
 }
 
-// One time step on stream st (no graph).
-int one_step(bgk_lattice* L, cudaStream_t st) {
+// One time step on stream st (no graph); with mom, the FP64 partial moments
+// of the new state go to mom (one slot of 5 doubles per block).
+int one_step(bgk_lattice* L, cudaStream_t st, double* mom = nullptr) {
     if (L->desc.pattern == BGK_PATTERN_AA) {
         const bool odd = (L->steps % 2) == 0;   // Layout E -> odd kernel
-        if (int e = aa_step(&L->p, L->a, odd, st)) return e;
+        if (int e = aa_step(&L->p, L->a, odd, mom, st)) return e;
     } else {
-        if (int e = sweep_launch(&L->p, L->a, L->b, st)) return e;
+        if (int e = sweep_launch_mom(&L->p, L->a, L->b, mom, st)) return e;
         for (int d = 0; d < 18; ++d) std::swap(L->a[d], L->b[d]);
     }
     ++L->steps;
@@ -253,6 +201,7 @@ int bgk_lattice_destroy(bgk_lattice* L) {
     if (L->base) cudaFree(L->base);
     if (L->obs_dev) cudaFree(L->obs_dev);
     if (L->ws) cudaFree(L->ws);
+    if (L->mom) cudaFree(L->mom);
     delete L;
     return BGK_OK;
 }
@@ -350,6 +299,28 @@ int bgk_lattice_step(bgk_lattice* L, int nsteps, void* stream) {
     while (left-- > 0)
         if (int e = one_step(L, st)) return e;
     return BGK_OK;
+}
+
+int bgk_lattice_step_moments(bgk_lattice* L, int nsteps, int every, double* out_dev, void* stream) {
+    if (!L || nsteps < 0 || every < 1 || !out_dev) return set_error(BGK_ERR_ARG, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long nb = sweep_blocks(&L->p, L->a[0]);
+    const size_t need = (size_t)nb * 5 * sizeof(double);
+    if (L->mom_bytes < need) {
+        if (L->mom) cudaFree(L->mom);
+        L->mom = nullptr; L->mom_bytes = 0;
+        cudaError_t e = cudaMalloc(&L->mom, need);
+        if (e != cudaSuccess) return set_error(BGK_ERR_NOMEM, "moment partials: %s", cudaGetErrorString(e));
+        L->mom_bytes = need;
+    }
+    const int samples = nsteps / every;
+    for (int s = 0; s < samples; ++s) {
+        if (every > 1)
+            if (int e = bgk_lattice_step(L, every - 1, stream)) return e;
+        if (int e = one_step(L, st, L->mom)) return e;
+        if (int e = finalize_moments(L->mom, nb, out_dev + 5 * (size_t)s, st)) return e;
+    }
+    return bgk_lattice_step(L, nsteps - samples * every, stream);
 }
 
 int bgk_lattice_set_omega(bgk_lattice* L, double omega) {

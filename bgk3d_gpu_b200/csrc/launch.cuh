@@ -1,0 +1,138 @@
+// Launch wrappers (templates) of every kernel, instantiated once per storage
+// kind by the inst_*.cu translation units; declared in kernels.h.
+#pragma once
+#include <cuda_runtime.h>
+#include "bgk3d_b200.h"
+#include "bgk_internal.h"
+#include "host_args.cuh"
+#include "sweep_ab.cuh"
+#include "sweep_aa.cuh"
+#include "reduce.cuh"
+
+namespace bgk {
+
+template <class S, class C, int BC>
+void launch_sweep_bc(const SweepArgs<S, C>& A, long long nelem, unsigned blocks, bool generic,
+                     cudaStream_t st) {
+    if (nelem < (1LL << 31)) {
+        if (generic) sweep_ab_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
+        else sweep_ab_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
+    } else {
+        if (generic) sweep_ab_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
+        else sweep_ab_kernel<S, C, BC, long long, false><<<blocks, 256, 0, st>>>(A);
+    }
+}
+
+template <class S, class C>
+int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st) {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
+    segment_geometry(A, a[0]);
+    A.mom = mom;
+    if (p->bcase == BC_INFLOW) {
+        dim3 blk(128), grd((p->m + 127) / 128, p->n);
+        outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
+        if (int e = check_launch("outflow_halo_kernel")) return e;
+    }
+    const long long warps = (long long)A.nseg * p->m * p->n;
+    const long long blocks = (warps + 7) / 8;
+    if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
+    const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
+    const bool g = generic_collision(p);
+    const unsigned nb = (unsigned)blocks;
+    switch (p->bcase) {
+        case BC_NONE: launch_sweep_bc<S, C, BC_NONE>(A, nelem, nb, g, st); break;
+        case BC_DRIVEN: launch_sweep_bc<S, C, BC_DRIVEN>(A, nelem, nb, g, st); break;
+        case BC_PERIODIC: launch_sweep_bc<S, C, BC_PERIODIC>(A, nelem, nb, g, st); break;
+        case BC_CHANNEL: launch_sweep_bc<S, C, BC_CHANNEL>(A, nelem, nb, g, st); break;
+        case BC_INFLOW: launch_sweep_bc<S, C, BC_INFLOW>(A, nelem, nb, g, st); break;
+    }
+    return check_launch("sweep_ab_kernel");
+}
+
+template <class S, class C>
+int launch_moments(const bgk_sweep_params* p, void* const* a, double* out, double* ws, cudaStream_t st) {
+    FieldArgs<S, C> F = field_args<S, C>(p, a);
+    dim3 grd, blk;
+    moments_grid(p->l, p->m, p->n, grd, blk);
+    moments_partial_kernel<S, C><<<grd, blk, 0, st>>>(F, ws);
+    if (int e = check_launch("moments_partial_kernel")) return e;
+    const long long nparts = (long long)grd.x * grd.y * grd.z;
+    finalize_partials_kernel<5><<<1, 256, 0, st>>>(ws, nparts, out);
+    return check_launch("finalize_partials_kernel");
+}
+
+template <class S, class C>
+int launch_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks, int ke,
+                    double* out, double* ws, size_t ws_bytes, cudaStream_t st) {
+    FieldArgs<S, C> F = field_args<S, C>(p, a);
+    const int ni = ie - is + 1, nj = je - js + 1, nk = ke - ks + 1;
+    const long long tot = (long long)ni * nj * nk;
+    const long long nb = (tot + 255) / 256;
+    if ((size_t)nb * 3 * sizeof(double) > ws_bytes)
+        return set_error(BGK_ERR_ARG, "draglift box needs %lld bytes of workspace", nb * 3 * 8);
+    draglift_partial_kernel<S, C><<<(unsigned)nb, 256, 0, st>>>(F, is, js, ks, ni, nj, nk, ws);
+    if (int e = check_launch("draglift_partial_kernel")) return e;
+    finalize_partials_kernel<3><<<1, 256, 0, st>>>(ws, nb, out);
+    return check_launch("finalize_partials_kernel");
+}
+
+template <class S, class C, int BC>
+void launch_aa_bc(const SweepArgs<S, C>& A, bool odd, bool generic, long long nelem, unsigned blocks,
+                  cudaStream_t st) {
+    if (nelem < (1LL << 31)) {
+        if (odd) {
+            if (generic) aa_odd_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
+            else aa_odd_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
+        } else {
+            if (generic) aa_even_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
+            else aa_even_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
+        }
+    } else {
+        if (odd) aa_odd_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
+        else aa_even_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
+    }
+}
+
+template <class S, class C>
+int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st) {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, slots, slots);
+    A.b[18] = (S*)slots[18];
+    segment_geometry(A, slots[0]);
+    A.mom = mom;
+    const long long warps = (long long)A.nseg * p->m * p->n;
+    if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
+    const unsigned blocks = (unsigned)((warps + 7) / 8);
+    const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
+    const bool g = generic_collision(p);
+    switch (p->bcase) {
+        case BC_DRIVEN: launch_aa_bc<S, C, BC_DRIVEN>(A, odd, g, nelem, blocks, st); break;
+        case BC_PERIODIC: launch_aa_bc<S, C, BC_PERIODIC>(A, odd, g, nelem, blocks, st); break;
+        case BC_CHANNEL: launch_aa_bc<S, C, BC_CHANNEL>(A, odd, g, nelem, blocks, st); break;
+        case BC_INFLOW: launch_aa_bc<S, C, BC_INFLOW>(A, odd, g, nelem, blocks, st); break;
+        default: return set_error(BGK_ERR_ARG, "AA lattices need a boundary case");
+    }
+    return check_launch(odd ? "aa_odd_kernel" : "aa_even_kernel");
+}
+
+template <class S, class C>
+int launch_aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, slots, slots);
+    dim3 blk(128), grd((p->m + 127) / 128, p->n);
+    aa_outflow_prepass_kernel<S, C><<<grd, blk, 0, st>>>(A);
+    return check_launch("aa_outflow_prepass_kernel");
+}
+
+}  // namespace bgk
+
+#define BGK_INSTANTIATE(S, C)                                                                      \
+    namespace bgk {                                                                                \
+    template int launch_sweep<S, C>(const bgk_sweep_params*, void* const*, void* const*, double*,  \
+                                    cudaStream_t);                                                 \
+    template int launch_moments<S, C>(const bgk_sweep_params*, void* const*, double*, double*,     \
+                                      cudaStream_t);                                               \
+    template int launch_draglift<S, C>(const bgk_sweep_params*, void* const*, int, int, int, int,  \
+                                       int, int, double*, double*, size_t, cudaStream_t);          \
+    template int launch_aa<S, C>(const bgk_sweep_params*, void* const*, bool, double*,             \
+                                 cudaStream_t);                                                    \
+    template int launch_aa_prepass<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);     \
+    }

@@ -42,6 +42,23 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NQ], double* part
     }
 }
 
+// Per-node diagnostics of SRC/diagno.F90:112-127 (rho, u in the compute
+// type) accumulated into FP64: v += {rho, u_x, u_y, u_z, 0.5|u|^2}.
+template <class C>
+__device__ __forceinline__ void diagno_node(const C (&x)[19], C cte1, double (&v)[5]) {
+    const C rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] +
+                  x[11] + x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18] + cte1;
+    const C rhoinv = C(1) / rho;
+    const C xj = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * rhoinv;
+    const C yj = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * rhoinv;
+    const C zj = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * rhoinv;
+    v[0] += (double)rho;
+    v[1] += (double)xj;
+    v[2] += (double)yj;
+    v[3] += (double)zj;
+    v[4] += (double)(C(0.5) * (xj * xj + yj * yj + zj * zj));
+}
+
 template <class S, class C>
 __device__ __forceinline__ bool is_solid(const FieldArgs<S, C>& P, int i, int j, int k) {
     if (P.obs == nullptr || i < P.imin || i > P.imax || j < P.jmin || j > P.jmax || k < P.kmin ||
@@ -65,17 +82,7 @@ __global__ void __launch_bounds__(256) moments_partial_kernel(const FieldArgs<S,
             C x[19];
 #pragma unroll
             for (int d = 0; d < 19; ++d) x[d] = Conv<S, C>::ld(P.a[d][c], P.inv_scale);
-            const C rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] +
-                          x[10] + x[11] + x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18] + P.cte1;
-            const C rhoinv = C(1) / rho;
-            const C xj = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * rhoinv;
-            const C yj = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * rhoinv;
-            const C zj = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * rhoinv;
-            v[0] += (double)rho;
-            v[1] += (double)xj;
-            v[2] += (double)yj;
-            v[3] += (double)zj;
-            v[4] += (double)(C(0.5) * (xj * xj + yj * yj + zj * zj));
+            diagno_node<C>(x, P.cte1, v);
         }
     }
     block_reduce_store<5>(v, partial);

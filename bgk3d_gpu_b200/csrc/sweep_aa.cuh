@@ -74,7 +74,7 @@ __device__ __forceinline__ bool aa_node(const SweepArgs<S, C>& P, int& i, int& j
 
 // Even (local) step.  P.a and P.b both name the slot arrays.
 template <class S, class C, int BC, class IDX, bool GENERIC>
-__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(const SweepArgs<S, C> P) {
+__device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
     int i, j, k;
     IDX c;
     if (!aa_node<S, C, IDX>(P, i, j, k, c)) return;
@@ -93,20 +93,30 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(co
     for (int d = 0; d < 19; ++d) st[d] = Conv<S, C>::st(y[d], scl);
 #pragma unroll
     for (int d = 0; d < 19; ++d) f[opp_of(d)][c] = st[d];
-    if (BC == BC_INFLOW && i == P.l) {
+    if ((BC == BC_INFLOW && i == P.l) || P.mom != nullptr) {
         C s[19];
 #pragma unroll
         for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(st[d], inv);
-        C eq[5];
-        outflow_eq<C>(s, P.inflow_cte1, P.col, eq);
+        if (BC == BC_INFLOW && i == P.l) {
+            C eq[5];
+            outflow_eq<C>(s, P.inflow_cte1, P.col, eq);
 #pragma unroll
-        for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::st(eq[e], scl);
+            for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::st(eq[e], scl);
+        }
+        if (P.mom != nullptr) diagno_node<C>(s, P.col.cte1, m5);
     }
+}
+
+template <class S, class C, int BC, class IDX, bool GENERIC>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(const SweepArgs<S, C> P) {
+    double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    aa_even_node<S, C, BC, IDX, GENERIC>(P, m5);
+    if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 
 // Odd (pull + push) step.
 template <class S, class C, int BC, class IDX, bool GENERIC>
-__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(const SweepArgs<S, C> P) {
+__device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
     typedef Faces<BC> F;
     int i, j, k;
     IDX c;
@@ -180,6 +190,12 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(con
         }
     }
     f[18][c] = Conv<S, C>::st(y[18], scl);
+    if (P.mom != nullptr) {
+        C s[19];
+#pragma unroll
+        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(Conv<S, C>::st(y[d], scl), inv);
+        diagno_node<C>(s, P.col.cte1, m5);
+    }
     if (BC == BC_INFLOW && i == 1) {
 #pragma unroll
         for (int d = 0; d < 5; ++d)
@@ -200,6 +216,13 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(con
             f[d][off] = Conv<S, C>::st(eq[e], scl);
         }
     }
+}
+
+template <class S, class C, int BC, class IDX, bool GENERIC>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(const SweepArgs<S, C> P) {
+    double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    aa_odd_node<S, C, BC, IDX, GENERIC>(P, m5);
+    if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 
 // Outflow halo in slot form for a freshly loaded Layout E state: halo cell

@@ -29,6 +29,7 @@
 // copies would otherwise read solid-node garbage.
 #pragma once
 #include "d3q19.cuh"
+#include "reduce.cuh"
 
 namespace bgk {
 
@@ -51,6 +52,7 @@ template <class S, class C> struct SweepArgs {
     int nseg_aligned;      // 1 when every row starts on a segment boundary
     uint32_t nrows;        // m * n
     FastDiv div_seg, div_m;
+    double* mom;           // optional: per-block FP64 partial moments of the new state
 };
 
 // Equilibrium population p (0..4 -> 01..05) of the inflow face
@@ -114,7 +116,7 @@ __device__ __forceinline__ uint32_t obstacle_links(const SweepArgs<S, C>& P, int
 // make every store and every c_x = 0 load a whole number of 32-byte sectors.
 // One thread per node; blocks of 256 threads = 8 row segments.
 template <class S, class C, int BC, class IDX, bool GENERIC>
-__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) sweep_ab_kernel(const SweepArgs<S, C> P) {
+__device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
     typedef Faces<BC> F;
     const int lane = threadIdx.x & 31;
     const uint32_t gw = blockIdx.x * 8u + (threadIdx.x >> 5);
@@ -174,9 +176,28 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) sweep_ab_kernel(c
     C y[19];
     bgk_collide<C, GENERIC>(x, y, P.col);
     const float scl = P.scale;
+    S sv[19];
 #pragma unroll
-    for (int d = 0; d < 18; ++d) P.b[d][c] = Conv<S, C>::st(y[d], scl);
-    const_cast<S*>(P.a[18])[c] = Conv<S, C>::st(y[18], scl);
+    for (int d = 0; d < 19; ++d) sv[d] = Conv<S, C>::st(y[d], scl);
+#pragma unroll
+    for (int d = 0; d < 18; ++d) P.b[d][c] = sv[d];
+    const_cast<S*>(P.a[18])[c] = sv[18];
+    if (P.mom != nullptr) {
+        C s[19];
+#pragma unroll
+        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(sv[d], inv);
+        diagno_node<C>(s, P.col.cte1, m5);
+    }
+}
+
+// One launch = one time step.  With P.mom set, every block also writes the
+// FP64 sums of SRC/diagno.F90's per-node moments of the state it produced
+// (fluid nodes) to P.mom[blockIdx.x * 5 ..].
+template <class S, class C, int BC, class IDX, bool GENERIC>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) sweep_ab_kernel(const SweepArgs<S, C> P) {
+    double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    sweep_node<S, C, BC, IDX, GENERIC>(P, m5);
+    if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 
 // Outflow halo plane for the inflow case: a10..a14(l+1, j, k) from the

@@ -197,6 +197,15 @@ class Lattice:
     def step(self, nsteps=1) -> None:
         check(self.L.bgk_lattice_step(self.h, int(nsteps), self._stream()), "bgk_lattice_step")
 
+    def step_moments(self, nsteps: int, every: int = 1) -> np.ndarray:
+        """Advance nsteps steps; FP64 moments of the state after every `every`-th
+        step, computed in the same pass as that step: array (nsteps // every, 5)."""
+        ns = nsteps // every
+        out = torch.zeros(max(ns, 1) * 5, dtype=torch.float64, device=self.device)
+        check(self.L.bgk_lattice_step_moments(self.h, int(nsteps), int(every), out.data_ptr(),
+                                              self._stream()), "bgk_lattice_step_moments")
+        return out[:ns * 5].view(ns, 5).cpu().numpy()
+
     @property
     def steps(self) -> int:
         return int(self.L.bgk_lattice_steps(self.h))

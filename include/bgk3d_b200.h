@@ -83,6 +83,14 @@ void bgk_sweep_params_init(bgk_sweep_params* p, int kind, int l, int m, int n, d
    outflow halo plane a[9..13](l+1, 1..m, 1..n). */
 int bgk_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, void* stream);
 
+/* bgk_sweep plus, in the same pass, the FP64 moments of the state it writes
+   (the sums bgk_moments would return on that state, up to FP64 summation
+   order) into out_dev[0..4].  Workspace: bgk_sweep_moments_workspace_bytes(p)
+   bytes of device memory (per-block partial sums). */
+size_t bgk_sweep_moments_workspace_bytes(const bgk_sweep_params* p);
+int bgk_sweep_moments(const bgk_sweep_params* p, void* const* a, void* const* b, double* out_dev,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* Bytes of device workspace bgk_moments / bgk_draglift need for a lattice of
    these extents (per-block FP64 partial sums). */
 size_t bgk_reduce_workspace_bytes(int l, int m, int n);
@@ -112,6 +120,13 @@ size_t bgk_moments_noalloc_max_bytes(void);
    (SRC/draglift.F90:77-176) into out_dev[0..2]. */
 int bgk_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
                  int ke, double* out_dev, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Helpers of the drop-in library's tracked moments (bgk3d_dropin.h):
+   bgk_sweep with per-block partial moments into partials (when they fit;
+   *nparts = number of partials written, 0 if not), and their second pass. */
+int bgk_dropin_sweep_tracked(const bgk_sweep_params* p, void* const* a, void* const* b, double* partials,
+                             size_t bytes, long long* nparts);
+int bgk_dropin_finalize(const double* partials, long long nparts, double* out_dev, void* stream);
 
 /* cudaDeviceSynchronize; returns BGK_ERR_CUDA (does not abort) on failure. */
 int bgk_device_sync(void);

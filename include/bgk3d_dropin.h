@@ -65,6 +65,15 @@ void gpu_device_sync(void);
    calling thread (e.g. after the caller re-allocates its arrays). */
 void bgk_dropin_reset(void);
 
+/* Not in the reference: with tracking on, every col_mc_gpu also sums the
+   FP64 moments of the state it writes (rho, u_x, u_y, u_z, 0.5|u|^2 over
+   the fluid nodes, the per-node arithmetic of SRC/diagno.F90), in the same pass;
+   bgk_dropin_moments then writes the last call's sums to out_dev[0..4]
+   (device memory) without reading the lattice again.  Returns 0, or
+   BGK_ERR_STATE (-5) when no tracked step exists. */
+void bgk_dropin_track_moments(int on);
+int bgk_dropin_moments(double* out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,11 @@ int bgk_lattice_store(const bgk_lattice* lat, void* host, void* stream);
    Runs of 16 or more steps replay a captured CUDA graph. */
 int bgk_lattice_step(bgk_lattice* lat, int nsteps, void* stream);
 
+/* Advance nsteps steps and record the FP64 moments (as bgk_moments) of the
+   state after every `every`-th step, computed in the same pass as that step:
+   sample s (0 <= s < nsteps / every) goes to out_dev[5 s .. 5 s + 4]. */
+int bgk_lattice_step_moments(bgk_lattice* lat, int nsteps, int every, double* out_dev, void* stream);
+
 /* Change the relaxation frequency / force of an existing lattice. */
 int bgk_lattice_set_omega(bgk_lattice* lat, double omega);
 
