@@ -16,7 +16,30 @@ class LatticeDesc(Structure):
     ]
 
 
+def bind_batch(L) -> None:
+    from ctypes import POINTER as P_
+    L.bgk_batch_create.argtypes = [P_(c_void_p), c_int, P_(c_void_p)]
+    L.bgk_batch_create.restype = c_int
+    L.bgk_batch_destroy.argtypes = [c_void_p]
+    L.bgk_batch_destroy.restype = c_int
+    L.bgk_batch_resync.argtypes = [c_void_p]
+    L.bgk_batch_resync.restype = c_int
+    L.bgk_batch_step.argtypes = [c_void_p, c_int, c_void_p]
+    L.bgk_batch_step.restype = c_int
+    L.bgk_batch_set_config.argtypes = [c_void_p, c_int, c_int]
+    L.bgk_batch_set_config.restype = c_int
+    L.bgk_batch_get_config.argtypes = [c_void_p, P_(c_int), P_(c_int)]
+    L.bgk_batch_get_config.restype = c_int
+    L.bgk_batch_tune.argtypes = [c_void_p, c_int, c_void_p, P_(c_int)]
+    L.bgk_batch_tune.restype = c_int
+    L.bgk_batch_nodes.argtypes = [c_void_p]
+    L.bgk_batch_nodes.restype = c_longlong
+    L.bgk_batch_tiles.argtypes = [c_void_p]
+    L.bgk_batch_tiles.restype = c_longlong
+
+
 def bind(L) -> None:
+    bind_batch(L)
     D = POINTER(LatticeDesc)
     L.bgk_lattice_desc_init.argtypes = [D, c_int, c_int, c_int, c_int, c_int, c_double]
     L.bgk_lattice_desc_init.restype = None

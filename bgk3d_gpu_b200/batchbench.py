@@ -1,0 +1,137 @@
+"""Batched sweep benchmark: many independent lattices of uneven sizes.
+
+Workload (seeded): `count` cubes with sides drawn from {32,48,64,96,128,160},
+tau uniform in [0.52, 0.8]; half Kida vortex (periodic, u0 = 0.05), half
+Poiseuille channel (x, y periodic, z walls, body force g = 1e-6 as g/10 per
+population with c_x != 0, times rho); FP32; `steps` steps each.
+
+Three ways to run the same solves are timed (CUDA events, same stream):
+  batched     one persistent tile-queue launch per step for all lattices,
+              16-step CUDA graphs, tile shape / grid chosen by the autotuner;
+  sequential  one lattice after another, each with its own launches replayed
+              through that lattice's CUDA graph;
+  plain       one lattice after another, one API call (= one launch) per step.
+All three give bit-identical final states (checked on every lattice).
+
+  python -m bgk3d_gpu_b200.batchbench [--count 96] [--steps 2000] [--seed 20261203]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+import torch
+
+from . import cases as CS
+from .lattice import Batch
+
+SIDES = (32, 48, 64, 96, 128, 160)
+
+
+def make_specs(count: int, seed: int):
+    rng = np.random.default_rng(seed)
+    sides = rng.choice(SIDES, size=count)
+    taus = rng.uniform(0.52, 0.8, size=count)
+    specs = []
+    for i in range(count):
+        n, tau = int(sides[i]), float(taus[i])
+        specs.append(CS.kida(n, tau, kind="f32") if i % 2 == 0 else CS.poiseuille(n, tau, kind="f32"))
+    return specs
+
+
+def build(specs):
+    lats, states = [], []
+    for c in specs:
+        lats.append(CS.make_lattice(c))
+        states.append(CS.initial_state(c, 1))
+    return lats, states
+
+
+def reload(lats, states):
+    for lat, st in zip(lats, states):
+        lat.upload(st)
+
+
+def timed(fn):
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    fn()
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3
+
+
+def run(count: int = 96, steps: int = 2000, seed: int = 20261203, modes=("batched", "sequential", "plain"),
+        tune_steps: int = 4):
+    specs = make_specs(count, seed)
+    lats, states = build(specs)
+    nodes = sum(c["l"] * c["m"] * c["n"] for c in specs)
+    out = {"workload": f"{count} lattices, sides {SIDES} seed {seed}, half Kida / half Poiseuille, FP32",
+           "lattices": count, "steps": steps, "nodes": nodes,
+           "device_gb": round(sum(lat.device_bytes for lat in lats) / 1e9, 2)}
+    finals = None
+    if "batched" in modes:
+        batch = Batch(lats)
+        used = batch.tune(tune_steps)
+        cfg = batch.config
+        out["tuned_config"] = {"tiles_per_grab": cfg[0], "blocks_per_sm": cfg[1], "tuning_steps": used}
+        reload(lats, states)
+        batch.resync()
+        t = timed(lambda: batch.step(steps))
+        finals = [lat.download() for lat in lats]
+        batch.close()
+        out["batched"] = {"seconds": t, "solves_per_s": count / t, "glups": nodes * steps / t / 1e9}
+    if "sequential" in modes:
+        reload(lats, states)
+        for lat in lats[:2]:
+            lat.step(32)                 # capture graphs outside the timed region
+        reload(lats, states)
+
+        def seq():
+            for lat in lats:
+                lat.step(steps)
+        t = timed(seq)
+        out["sequential"] = {"seconds": t, "solves_per_s": count / t, "glups": nodes * steps / t / 1e9}
+        if finals is not None:
+            out["sequential"]["identical_to_batched"] = all(
+                np.array_equal(f, lat.download()) for f, lat in zip(finals, lats))
+    if "plain" in modes:
+        reload(lats, states)
+
+        def plain():
+            for lat in lats:
+                for _ in range(steps):
+                    lat.step(1)
+        t = timed(plain)
+        out["plain"] = {"seconds": t, "solves_per_s": count / t, "glups": nodes * steps / t / 1e9}
+        if finals is not None:
+            out["plain"]["identical_to_batched"] = all(
+                np.array_equal(f, lat.download()) for f, lat in zip(finals, lats))
+    if "batched" in out:
+        for k in ("sequential", "plain"):
+            if k in out:
+                out[f"batched_vs_{k}"] = out["batched"]["solves_per_s"] / out[k]["solves_per_s"]
+    for lat in lats:
+        lat.close()
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--count", type=int, default=96)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--modes", default="batched,sequential,plain")
+    args = ap.parse_args(argv)
+    res = run(args.count, args.steps, args.seed, tuple(args.modes.split(",")))
+    print(json.dumps(res), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,114 @@
+// Batched time step: many independent lattices of different extents,
+// boundary cases and collision parameters advanced by ONE persistent launch.
+//
+// Work is cut into tiles of 8 row segments (256 nodes, one block's worth in
+// the single-lattice sweep).  Tiles of all lattices are numbered
+// consecutively (tile_begin[L] is lattice L's first tile); a persistent grid
+// of blocks takes `sub` consecutive tiles at a time from a device counter
+// (the tile queue), finds the tile's lattice by binary search, stages that
+// lattice's kernel arguments in shared memory, and runs the same per-node
+// code as sweep_ab_kernel for the lattice's boundary case.  The last block
+// to finish resets the counter, so the next launch (or graph replay) starts
+// from an empty queue with no host intervention.
+#pragma once
+#include "sweep_ab.cuh"
+
+namespace bgk {
+
+template <class S, class C> struct BatchView {
+    const SweepArgs<S, C>* desc;   // 2 per lattice: [2 L + parity], parity 1 = a/b swapped
+    const uint32_t* tile_begin;    // nlat + 1 entries
+    int nlat;
+    uint32_t ntiles;
+    unsigned* counter;             // [0] next tile, [1] blocks finished
+    int parity;
+    int sub;                       // tiles taken per queue access
+};
+
+template <class S, class C>
+__device__ __forceinline__ void batch_node(const SweepArgs<S, C>& P, uint32_t gw) {
+    double m5[5];
+    const bool g = P.generic != 0;
+    switch (P.bcase) {
+        case BC_DRIVEN:
+            if (g) sweep_node<S, C, BC_DRIVEN, int, true>(P, gw, m5);
+            else sweep_node<S, C, BC_DRIVEN, int, false>(P, gw, m5);
+            break;
+        case BC_PERIODIC:
+            if (g) sweep_node<S, C, BC_PERIODIC, int, true>(P, gw, m5);
+            else sweep_node<S, C, BC_PERIODIC, int, false>(P, gw, m5);
+            break;
+        case BC_CHANNEL:
+            if (g) sweep_node<S, C, BC_CHANNEL, int, true>(P, gw, m5);
+            else sweep_node<S, C, BC_CHANNEL, int, false>(P, gw, m5);
+            break;
+        case BC_INFLOW:
+            if (g) sweep_node<S, C, BC_INFLOW, int, true>(P, gw, m5);
+            else sweep_node<S, C, BC_INFLOW, int, false>(P, gw, m5);
+            break;
+        default: break;
+    }
+}
+
+template <class S, class C>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) batch_sweep_kernel(const BatchView<S, C> V) {
+    __shared__ __align__(16) SweepArgs<S, C> sd;
+    __shared__ uint32_t s_tile;
+    __shared__ int s_lat;
+    int cur = -1;
+    const uint32_t warp = threadIdx.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(V.counter, (unsigned)V.sub);
+        __syncthreads();
+        const uint32_t t0 = s_tile;
+        if (t0 >= V.ntiles) break;
+        const uint32_t t1 = min(t0 + (uint32_t)V.sub, V.ntiles);
+        for (uint32_t t = t0; t < t1; ++t) {
+            if (threadIdx.x == 0) {
+                int lo = 0, hi = V.nlat - 1;   // last L with tile_begin[L] <= t
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (__ldg(V.tile_begin + mid) <= t) lo = mid; else hi = mid - 1;
+                }
+                s_lat = lo;
+            }
+            __syncthreads();
+            const int L = s_lat;
+            if (L != cur) {
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(V.desc + 2 * L + V.parity);
+                uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+                for (uint32_t w = threadIdx.x; w < sizeof(SweepArgs<S, C>) / 4; w += blockDim.x) dst[w] = __ldg(src + w);
+                cur = L;
+                __syncthreads();
+            }
+            batch_node<S, C>(sd, (t - __ldg(V.tile_begin + L)) * 8u + warp);
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned done = atomicAdd(V.counter + 1, 1u);
+        if (done == gridDim.x - 1) {   // every block has left the queue
+            V.counter[0] = 0u;
+            V.counter[1] = 0u;
+            __threadfence();
+        }
+    }
+}
+
+// Non-persistent variant: one block per tile (the hardware block scheduler is
+// the queue); the tile's lattice is found by every thread, and its kernel
+// arguments are read through the L1 cache.
+template <class S, class C>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) batch_grid_kernel(const BatchView<S, C> V) {
+    const uint32_t t = blockIdx.x;
+    int lo = 0, hi = V.nlat - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(V.tile_begin + mid) <= t) lo = mid; else hi = mid - 1;
+    }
+    const SweepArgs<S, C>& P = V.desc[2 * lo + V.parity];
+    batch_node<S, C>(P, (t - __ldg(V.tile_begin + lo)) * 8u + (threadIdx.x >> 5));
+}
+
+}  // namespace bgk

@@ -19,6 +19,13 @@ template <class S, class C>
 int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st);
 template <class S, class C>
 int launch_aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st);
+template <class S, class C>
+size_t fill_batch_desc(const bgk_sweep_params* p, void* const* a, void* const* b, void* out, uint32_t* tiles);
+template <class S, class C>
+int launch_batch(const void* desc, const uint32_t* tile_begin, int nlat, uint32_t ntiles, unsigned* counter,
+                 int parity, int sub, int grid, cudaStream_t st);
+template <class S, class C>
+int launch_outflow(const bgk_sweep_params* p, void* const* a, cudaStream_t st);
 }  // namespace bgk
 
 // storage kinds: 0 f64/f64, 1 f32/f32, 2 f16/f32, 3 bf16/f32, 4 f32/f64

@@ -8,6 +8,7 @@
 #include "sweep_ab.cuh"
 #include "sweep_aa.cuh"
 #include "reduce.cuh"
+#include "batch.cuh"
 
 namespace bgk {
 
@@ -122,6 +123,51 @@ int launch_aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_
     return check_launch("aa_outflow_prepass_kernel");
 }
 
+// Batched stepping (batch.cuh): the two kernel-argument records of one
+// lattice (parity 0: current a/b, parity 1: swapped) and its tile count.
+template <class S, class C>
+size_t fill_batch_desc(const bgk_sweep_params* p, void* const* a, void* const* b, void* out, uint32_t* tiles) {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
+    segment_geometry(A, a[0]);
+    SweepArgs<S, C> B = A;
+    for (int d = 0; d < 18; ++d) {
+        B.a[d] = (const S*)b[d];
+        B.b[d] = (S*)a[d];
+    }
+    SweepArgs<S, C>* o = static_cast<SweepArgs<S, C>*>(out);
+    o[0] = A;
+    o[1] = B;
+    *tiles = (uint32_t)(((long long)A.nseg * p->m * p->n + 7) / 8);
+    return 2 * sizeof(SweepArgs<S, C>);
+}
+
+template <class S, class C>
+int launch_batch(const void* desc, const uint32_t* tile_begin, int nlat, uint32_t ntiles, unsigned* counter,
+                 int parity, int sub, int grid, cudaStream_t st) {
+    BatchView<S, C> V;
+    V.desc = static_cast<const SweepArgs<S, C>*>(desc);
+    V.tile_begin = tile_begin;
+    V.nlat = nlat;
+    V.ntiles = ntiles;
+    V.counter = counter;
+    V.parity = parity;
+    V.sub = sub;
+    if (grid <= 0) {   // one block per tile
+        batch_grid_kernel<S, C><<<ntiles, 256, 0, st>>>(V);
+        return check_launch("batch_grid_kernel");
+    }
+    batch_sweep_kernel<S, C><<<grid, 256, 0, st>>>(V);
+    return check_launch("batch_sweep_kernel");
+}
+
+template <class S, class C>
+int launch_outflow(const bgk_sweep_params* p, void* const* a, cudaStream_t st) {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, a, a);
+    dim3 blk(128), grd((p->m + 127) / 128, p->n);
+    outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
+    return check_launch("outflow_halo_kernel");
+}
+
 }  // namespace bgk
 
 #define BGK_INSTANTIATE(S, C)                                                                      \
@@ -135,4 +181,9 @@ int launch_aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_
     template int launch_aa<S, C>(const bgk_sweep_params*, void* const*, bool, double*,             \
                                  cudaStream_t);                                                    \
     template int launch_aa_prepass<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);     \
+    template size_t fill_batch_desc<S, C>(const bgk_sweep_params*, void* const*, void* const*,     \
+                                          void*, uint32_t*);                                       \
+    template int launch_batch<S, C>(const void*, const uint32_t*, int, uint32_t, unsigned*, int,   \
+                                    int, int, cudaStream_t);                                       \
+    template int launch_outflow<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);        \
     }

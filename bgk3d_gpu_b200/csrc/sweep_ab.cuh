@@ -53,6 +53,8 @@ template <class S, class C> struct SweepArgs {
     uint32_t nrows;        // m * n
     FastDiv div_seg, div_m;
     double* mom;           // optional: per-block FP64 partial moments of the new state
+    int bcase;             // BC_* (used by the batched kernel, which dispatches per tile)
+    int generic;           // 1 unless the force-free shifted collision applies
 };
 
 // Equilibrium population p (0..4 -> 01..05) of the inflow face
@@ -115,11 +117,11 @@ __device__ __forceinline__ uint32_t obstacle_links(const SweepArgs<S, C>& P, int
 // 32; a row starting mid-segment simply leaves lanes idle).  Aligned warps
 // make every store and every c_x = 0 load a whole number of 32-byte sectors.
 // One thread per node; blocks of 256 threads = 8 row segments.
+// gw: this warp's global segment index within the lattice.
 template <class S, class C, int BC, class IDX, bool GENERIC>
-__device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
+__device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
     typedef Faces<BC> F;
     const int lane = threadIdx.x & 31;
-    const uint32_t gw = blockIdx.x * 8u + (threadIdx.x >> 5);
     const uint32_t row = P.div_seg.div(gw);
     if (row >= P.nrows) return;
     const int seg = (int)(gw - row * (uint32_t)P.nseg);
@@ -196,7 +198,7 @@ __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, double (&m5
 template <class S, class C, int BC, class IDX, bool GENERIC>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) sweep_ab_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    sweep_node<S, C, BC, IDX, GENERIC>(P, m5);
+    sweep_node<S, C, BC, IDX, GENERIC>(P, blockIdx.x * 8u + (threadIdx.x >> 5), m5);
     if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 

@@ -218,3 +218,57 @@ class Lattice:
         check(self.L.bgk_lattice_draglift(self.h, *[int(v) for v in box], self._out.data_ptr(),
                                           self._stream()), "draglift")
         return self._out[:3].cpu().numpy().copy()
+
+
+class Batch:
+    """Many Lattice objects (AB pattern, one storage kind) advanced together by
+    one persistent launch per step over a device tile queue (bgk_batch_*)."""
+
+    def __init__(self, lattices):
+        self.L = lib()
+        self.members = list(lattices)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.h.value for m in self.members])
+        h = ctypes.c_void_p()
+        check(self.L.bgk_batch_create(arr, len(self.members), ctypes.byref(h)), "bgk_batch_create")
+        self.h = h
+        self.device = self.members[0].device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bgk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def step(self, nsteps: int = 1) -> None:
+        check(self.L.bgk_batch_step(self.h, int(nsteps), self._stream()), "bgk_batch_step")
+
+    def resync(self) -> None:
+        """Accept members' states after they were loaded or stepped on their own."""
+        check(self.L.bgk_batch_resync(self.h), "bgk_batch_resync")
+
+    def tune(self, trial_steps: int = 4) -> int:
+        used = ctypes.c_int()
+        check(self.L.bgk_batch_tune(self.h, int(trial_steps), self._stream(), ctypes.byref(used)),
+              "bgk_batch_tune")
+        return used.value
+
+    @property
+    def config(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(self.L.bgk_batch_get_config(self.h, ctypes.byref(a), ctypes.byref(b)), "get_config")
+        return a.value, b.value
+
+    def set_config(self, tiles_per_grab: int, blocks_per_sm: int) -> None:
+        check(self.L.bgk_batch_set_config(self.h, tiles_per_grab, blocks_per_sm), "set_config")
+
+    @property
+    def nodes(self) -> int:
+        return int(self.L.bgk_batch_nodes(self.h))
