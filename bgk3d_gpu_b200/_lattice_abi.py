@@ -51,6 +51,8 @@ def bind(L) -> None:
     L.bgk_lattice_destroy.restype = c_int
     L.bgk_lattice_set_obstacle.argtypes = [c_void_p, c_void_p]
     L.bgk_lattice_set_obstacle.restype = c_int
+    L.bgk_lattice_init.argtypes = [c_void_p, c_int, c_void_p, c_void_p]
+    L.bgk_lattice_init.restype = c_int
     L.bgk_lattice_load.argtypes = [c_void_p, c_void_p, c_void_p]
     L.bgk_lattice_load.restype = c_int
     L.bgk_lattice_store.argtypes = [c_void_p, c_void_p, c_void_p]

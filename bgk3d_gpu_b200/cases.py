@@ -86,7 +86,8 @@ def lid_driven_cavity(n: int = 128, kind: str = "f64", re: float = 400.0, u_lid:
     nu = u_lid n / Re, rest initial state."""
     nu = u_lid * n / re
     return dict(l=n, m=n, n=n, kind=kind, bcase="driven", omega=1.0 / tau_from_nu(nu),
-                lid_force=u_lid / 6.0, init=_rest(n, n, n), nu=nu, name=f"ldc{n}_{kind}", **kw)
+                lid_force=u_lid / 6.0, init=_rest(n, n, n), flow=("rest", (1.0, 0.0, 0.0, 0.0)), nu=nu,
+                name=f"ldc{n}_{kind}", **kw)
 
 
 def taylor_green(n: int = 256, kind: str = "f32", u0: float = 0.05, re: float = 1600.0, **kw):
@@ -96,7 +97,7 @@ def taylor_green(n: int = 256, kind: str = "f32", u0: float = 0.05, re: float = 
     def init(device="cuda"):
         return F.taylor_green_fields(n, n, n, u0, device=device)
     return dict(l=n, m=n, n=n, kind=kind, bcase="periodic", omega=1.0 / tau_from_nu(nu), init=init,
-                nu=nu, u0=u0, name=f"tgv{n}_{kind}", **kw)
+                flow=("tgv", (u0,)), nu=nu, u0=u0, name=f"tgv{n}_{kind}", **kw)
 
 
 def kida(n: int, tau: float, kind: str = "f32", u0: float = 0.05, **kw):
@@ -104,7 +105,7 @@ def kida(n: int, tau: float, kind: str = "f32", u0: float = 0.05, **kw):
     def init(device="cuda"):
         return F.kida_fields(n, n, n, u0, device=device)
     return dict(l=n, m=n, n=n, kind=kind, bcase="periodic", omega=1.0 / tau, init=init,
-                name=f"kida{n}_{kind}", **kw)
+                flow=("kida", (u0,)), name=f"kida{n}_{kind}", **kw)
 
 
 def poiseuille(n: int, tau: float, kind: str = "f32", g: float = 1e-6, **kw):
@@ -113,7 +114,8 @@ def poiseuille(n: int, tau: float, kind: str = "f32", g: float = 1e-6, **kw):
     (SRC/col_MC.F90:501-518), 10 force per node and step, with
     force = fgrad * rho (:482); g / 10 per population gives momentum g rho."""
     return dict(l=n, m=n, n=n, kind=kind, bcase="channel", omega=1.0 / tau, force_mode=1,
-                force=(g / 10.0, 0.0, 0.0), init=_rest(n, n, n), name=f"pof{n}_{kind}", **kw)
+                force=(g / 10.0, 0.0, 0.0), init=_rest(n, n, n), flow=("rest", (1.0, 0.0, 0.0, 0.0)),
+                name=f"pof{n}_{kind}", **kw)
 
 
 def sphere(l: int = 512, m: int = 256, n: int = 256, kind: str = "f32", diameter: float = 40.0,
@@ -124,16 +126,18 @@ def sphere(l: int = 512, m: int = 256, n: int = 256, kind: str = "f32", diameter
     nu = u_in * diameter / re
     obs, bbox = solid_sphere_obstacle(l, m, n, diameter, center)
     return dict(l=l, m=m, n=n, kind=kind, bcase="inflow", omega=1.0 / tau_from_nu(nu), u_inflow=u_in,
-                init=_rest(l, m, n), obstacle=obs, drag_box=drag_box(bbox), radius=diameter / 2.0,
-                nu=nu, name=f"sphere{l}x{m}x{n}_{kind}", **kw)
+                init=_rest(l, m, n), flow=("rest", (1.0, 0.0, 0.0, 0.0)), obstacle=obs,
+                drag_box=drag_box(bbox), radius=diameter / 2.0, nu=nu, name=f"sphere{l}x{m}x{n}_{kind}", **kw)
 
 
 LATTICE_KEYS = ("kind", "bcase", "omega", "lid_force", "u_inflow", "force_mode", "force", "scale",
                 "pattern")
 
 
-def make_lattice(case: dict, pattern: str = "ab", scale: float | None = None):
-    """Create a Lattice for the case, load its initial state, set its obstacle."""
+def make_lattice(case: dict, pattern: str = "ab", scale: float | None = None, on_device: bool = True):
+    """Create a Lattice for the case, set its obstacle and its initial state:
+    computed on the device for the analytic flows (default), else built with
+    torch and loaded from the host."""
     import torch
     from .lattice import Lattice
     kw = {k: case[k] for k in LATTICE_KEYS if k in case}
@@ -145,7 +149,10 @@ def make_lattice(case: dict, pattern: str = "ab", scale: float | None = None):
     lat = Lattice(case["l"], case["m"], case["n"], **kw)
     if case.get("obstacle") is not None:
         lat.set_obstacle(case["obstacle"])
-    lat.upload(initial_state(case, lat.kind, kw.get("scale", 1.0)))
+    if on_device and case.get("flow") is not None:
+        lat.init_flow(*case["flow"])
+    else:
+        lat.upload(initial_state(case, lat.kind, kw.get("scale", 1.0)))
     return lat
 
 

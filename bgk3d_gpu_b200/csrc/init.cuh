@@ -1,0 +1,80 @@
+// On-device initial conditions: equilibrium populations of an analytic flow
+// written straight into a lattice (no host round trip), the device form of
+// SRC/init.F90:113-201.
+//
+// Flows (the BASELINE forms of the reference's cases):
+//   INIT_UNIFORM  rho = p[0], u = (p[1], p[2], p[3])   (rest: 1, 0, 0, 0)
+//   INIT_TGV      Taylor-Green: x = 2 pi (i-1)/l, ...,
+//                 u = u0 sin x cos y cos z, v = -u0 cos x sin y cos z, w = 0,
+//                 rho = 1 + 3 (u0^2/16)(cos 2x + cos 2y)(cos 2z + 2),  u0 = p[0]
+//   INIT_KIDA     Kida vortex, rho = 1,                  u0 = p[0]
+// Populations are f_p^eq - w_p = w_p (rho - 1) + w_p rho (3 c.u + 4.5 (c.u)^2
+// - 1.5 u^2) in double, rounded once to the storage kind.  (The reference's
+// init.F90 drops the w_p (rho - 1) term for shifted storage, :179-197.)
+#pragma once
+#include "d3q19.cuh"
+
+namespace bgk {
+
+enum InitFlow : int { INIT_UNIFORM = 0, INIT_TGV = 1, INIT_KIDA = 2 };
+
+template <class S> struct InitArgs {
+    S* f[19];            // destination arrays of populations 01..19 (AA: slot arrays already permuted)
+    long long nx, nxy;
+    int l, m, n;
+    int flow;
+    double p[4];
+    float scale;
+};
+
+__device__ __forceinline__ double weight_of(int d) {
+    const int s = abs(cx_of(d)) + abs(cy_of(d)) + abs(cz_of(d));
+    return s == 2 ? 1.0 / 36.0 : (s == 1 ? 1.0 / 18.0 : 1.0 / 3.0);
+}
+
+template <class S> __device__ __forceinline__ S store_from_double(double v, float scl);
+template <> __device__ __forceinline__ double store_from_double<double>(double v, float) { return v; }
+template <> __device__ __forceinline__ float store_from_double<float>(double v, float) { return __double2float_rn(v); }
+template <> __device__ __forceinline__ __half store_from_double<__half>(double v, float scl) {
+    return __float2half_rn(__fmul_rn(__double2float_rn(v), scl));
+}
+template <> __device__ __forceinline__ __nv_bfloat16 store_from_double<__nv_bfloat16>(double v, float scl) {
+    return __float2bfloat16_rn(__fmul_rn(__double2float_rn(v), scl));
+}
+
+// One thread per node (0..l+1, 0..m+1, 0..n+1): the halo gets the flow
+// evaluated at its own coordinates (periodic images coincide).
+template <class S>
+__global__ void init_equilibrium_kernel(const InitArgs<S> A) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long ni = A.l + 2, nj = A.m + 2, nk = A.n + 2;
+    if (t >= ni * nj * nk) return;
+    const int i = (int)(t % ni), j = (int)((t / ni) % nj), k = (int)(t / (ni * nj));
+    double rho = 1.0, ux = 0.0, uy = 0.0, uz = 0.0;
+    if (A.flow == INIT_UNIFORM) {
+        rho = A.p[0]; ux = A.p[1]; uy = A.p[2]; uz = A.p[3];
+    } else {
+        const double tp = 6.283185307179586476925286766559;
+        const double x = tp * (i - 1) / A.l, y = tp * (j - 1) / A.m, z = tp * (k - 1) / A.n;
+        const double u0 = A.p[0];
+        if (A.flow == INIT_TGV) {
+            ux = u0 * sin(x) * cos(y) * cos(z);
+            uy = -u0 * cos(x) * sin(y) * cos(z);
+            rho = 1.0 + 3.0 * (u0 * u0 / 16.0) * (cos(2.0 * x) + cos(2.0 * y)) * (cos(2.0 * z) + 2.0);
+        } else {
+            ux = u0 * sin(x) * (cos(3.0 * y) * cos(z) - cos(y) * cos(3.0 * z));
+            uy = u0 * sin(y) * (cos(3.0 * z) * cos(x) - cos(z) * cos(3.0 * x));
+            uz = u0 * sin(z) * (cos(3.0 * x) * cos(y) - cos(x) * cos(3.0 * y));
+        }
+    }
+    const double usq = ux * ux + uy * uy + uz * uz;
+    const long long c = i + A.nx * j + A.nxy * k;
+#pragma unroll
+    for (int d = 0; d < 19; ++d) {
+        const double cu = cx_of(d) * ux + cy_of(d) * uy + cz_of(d) * uz;
+        const double w = weight_of(d);
+        A.f[d][c] = store_from_double<S>(w * (rho - 1.0) + w * rho * (3.0 * cu + 4.5 * cu * cu - 1.5 * usq), A.scale);
+    }
+}
+
+}  // namespace bgk

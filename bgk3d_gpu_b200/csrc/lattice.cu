@@ -243,6 +243,36 @@ int bgk_lattice_load(bgk_lattice* L, const void* host, void* stream) {
     return BGK_OK;
 }
 
+int bgk_lattice_init(bgk_lattice* L, int flow, const double* params, void* stream) {
+    if (!L) return set_error(BGK_ERR_ARG, "null lattice");
+    if (flow < 0 || flow > 2) return set_error(BGK_ERR_ARG, "unknown flow %d", flow);
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int q = 0; q < 19; ++q) L->a[q] = L->planes[q];
+    if (L->desc.pattern == BGK_PATTERN_AB) {
+        for (int q = 0; q < 18; ++q) L->b[q] = L->planes[19 + q];
+        L->b[18] = L->a[18];
+    }
+    void* f[19];
+    for (int d = 0; d < 19; ++d) f[d] = (L->desc.pattern == BGK_PATTERN_AA) ? L->a[opp_of(d)] : L->a[d];
+    const float scale = (L->desc.kind == K_F16 || L->desc.kind == K_BF16) ? L->desc.scale : 1.0f;
+    int rc;
+    {
+        const bgk_sweep_params* p = &L->p;
+        switch (L->desc.kind) {
+            case K_F64: rc = launch_init<double, double>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
+            case K_F32: rc = launch_init<float, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
+            case K_F16: rc = launch_init<__half, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
+            case K_BF16: rc = launch_init<__nv_bfloat16, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
+            default: rc = launch_init<float, double>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
+        }
+    }
+    if (rc) return rc;
+    L->steps = 0;
+    if (L->desc.pattern == BGK_PATTERN_AA && L->desc.bcase == BC_INFLOW)
+        if (int e = aa_prepass(&L->p, L->a, st)) return e;
+    return BGK_OK;
+}
+
 int bgk_lattice_store(const bgk_lattice* L, void* host, void* stream) {
     if (!L || !host) return set_error(BGK_ERR_ARG, "null argument");
     if (L->desc.pattern == BGK_PATTERN_AA && (L->steps % 2) != 0)

@@ -9,6 +9,7 @@
 #include "sweep_aa.cuh"
 #include "reduce.cuh"
 #include "batch.cuh"
+#include "init.cuh"
 
 namespace bgk {
 
@@ -168,6 +169,21 @@ int launch_outflow(const bgk_sweep_params* p, void* const* a, cudaStream_t st) {
     return check_launch("outflow_halo_kernel");
 }
 
+template <class S, class C>
+int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n, int flow, const double* prm,
+                float scale, cudaStream_t st) {
+    InitArgs<S> A;
+    for (int d = 0; d < 19; ++d) A.f[d] = (S*)f[d];
+    A.nx = nx; A.nxy = nx * ny;
+    A.l = l; A.m = m; A.n = n;
+    A.flow = flow;
+    for (int q = 0; q < 4; ++q) A.p[q] = prm ? prm[q] : 0.0;
+    A.scale = scale;
+    const long long nodes = (long long)(l + 2) * (m + 2) * (n + 2);
+    init_equilibrium_kernel<S><<<(unsigned)((nodes + 255) / 256), 256, 0, st>>>(A);
+    return check_launch("init_equilibrium_kernel");
+}
+
 }  // namespace bgk
 
 #define BGK_INSTANTIATE(S, C)                                                                      \
@@ -186,4 +202,6 @@ int launch_outflow(const bgk_sweep_params* p, void* const* a, cudaStream_t st) {
     template int launch_batch<S, C>(const void*, const uint32_t*, int, uint32_t, unsigned*, int,   \
                                     int, int, cudaStream_t);                                       \
     template int launch_outflow<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);        \
+    template int launch_init<S, C>(void* const*, long long, long long, int, int, int, int,          \
+                                   const double*, float, cudaStream_t);                            \
     }

@@ -187,6 +187,13 @@ class Lattice:
         check(self.L.bgk_lattice_load(self.h, st.ctypes.data, self._stream()), "bgk_lattice_load")
         torch.cuda.current_stream(self.device).synchronize()
 
+    FLOWS = {"uniform": 0, "rest": 0, "tgv": 1, "kida": 2}
+
+    def init_flow(self, flow: str, params=(1.0, 0.0, 0.0, 0.0)) -> None:
+        """Equilibrium state of an analytic flow computed on the device."""
+        arr = (ctypes.c_double * 4)(*([float(v) for v in params] + [0.0] * (4 - len(params))))
+        check(self.L.bgk_lattice_init(self.h, self.FLOWS[flow], arr, self._stream()), "bgk_lattice_init")
+
     def download(self) -> np.ndarray:
         dt = {0: np.float64, 1: np.float32, 2: np.uint16, 3: np.uint16, 4: np.float32}[self.kind]
         out = np.empty((19, self.n + 2, self.m + 2, self.l + 2), dt)

@@ -61,6 +61,13 @@ int bgk_lattice_set_obstacle(bgk_lattice* lat, const int32_t* obs_host);
 int bgk_lattice_load(bgk_lattice* lat, const void* host, void* stream);
 int bgk_lattice_store(const bgk_lattice* lat, void* host, void* stream);
 
+/* Equilibrium initial state of an analytic flow computed on the device
+   (SRC/init.F90:113-201 without the host): flow 0 uniform (params = rho,
+   u_x, u_y, u_z; rest = 1,0,0,0), 1 Taylor-Green vortex (params[0] = u0;
+   x = 2 pi (i-1)/l, ...), 2 Kida vortex (params[0] = u0, rho = 1).  Resets the
+   step count like bgk_lattice_load. */
+int bgk_lattice_init(bgk_lattice* lat, int flow, const double* params, void* stream);
+
 /* Advance nsteps time steps (boundaries + stream + collide), stream-ordered.
    Runs of 16 or more steps replay a captured CUDA graph. */
 int bgk_lattice_step(bgk_lattice* lat, int nsteps, void* stream);

@@ -31,10 +31,14 @@ def _alone(req):
     return st, m
 
 
-def test_results_identical_alone_and_in_the_mix():
+@pytest.mark.parametrize("mode,floor", [("continuous", 8e6), ("continuous", 3e4), ("shared", 0)])
+def test_results_identical_alone_and_in_the_mix(mode, floor):
+    """floor 3e4 nodes makes the shortest-work-first policy step only a few
+    solves per round, so batches change membership between rounds."""
     from bgk3d_gpu_b200.serve import Server
     trace = _trace()
-    done, summary = Server(budget_bytes=20e9, max_chunk=25).run(trace, keep_states=True)
+    done, summary = Server(budget_bytes=20e9, max_chunk=25, floor_nodes=floor).run(trace, mode=mode,
+                                                                                 keep_states=True)
     assert summary["requests"] == len(trace)
     assert summary["rounds"] > len(trace)       # solves shared rounds
     by_id = {d["rid"]: d for d in done}
@@ -46,6 +50,23 @@ def test_results_identical_alone_and_in_the_mix():
         assert got["latency"] >= 0
     assert summary["p99_latency_s"] >= summary["p50_latency_s"] > 0
     assert summary["aggregate_glups"] > 0
+
+
+def test_shortest_work_first_selection():
+    from bgk3d_gpu_b200.serve import Server
+
+    class A:
+        def __init__(self, rid, remaining, nodes):
+            self.req = type("R", (), {"arrival": float(rid)})()
+            self.remaining, self.nodes = remaining, nodes
+
+    acts = [A(0, 1000, 10), A(1, 10, 100), A(2, 500, 5), A(3, 10, 100)]
+    srv = Server.__new__(Server)
+    srv.floor_nodes = 150
+    sel = srv.select(acts, "continuous")
+    # work: 10000, 1000, 2500, 1000 -> ids 1, 3 (ties by arrival) reach 200 >= 150
+    assert [a.req.arrival for a in sel] == [1.0, 3.0]
+    assert srv.select(acts, "shared") == acts
 
 
 def test_fifo_mode_and_memory_budget():
