@@ -1,6 +1,8 @@
 """ctypes signatures of the library-owned lattice entry points (include/bgk3d_lattice.h)."""
 from __future__ import annotations
 
+import ctypes
+
 from ctypes import (POINTER, Structure, c_double, c_float, c_int, c_longlong, c_size_t, c_void_p)
 
 
@@ -51,6 +53,18 @@ def bind(L) -> None:
     L.bgk_lattice_destroy.restype = c_int
     L.bgk_lattice_set_obstacle.argtypes = [c_void_p, c_void_p]
     L.bgk_lattice_set_obstacle.restype = c_int
+    L.bgk_lattice_save.argtypes = [c_void_p, ctypes.c_char_p, c_int, c_int, c_void_p]
+    L.bgk_lattice_save.restype = c_int
+    L.bgk_lattice_restore.argtypes = [c_void_p, ctypes.c_char_p, ctypes.POINTER(c_int), c_void_p]
+    L.bgk_lattice_restore.restype = c_int
+    L.bgk_io_set_subrecord_limit.argtypes = [ctypes.c_longlong]
+    L.bgk_io_set_subrecord_limit.restype = ctypes.c_longlong
+    L.bgk_lattice_profile.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]
+    L.bgk_lattice_profile.restype = c_int
+    L.bgk_lattice_probe.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]
+    L.bgk_lattice_probe.restype = c_int
+    L.bgk_lattice_slice.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p]
+    L.bgk_lattice_slice.restype = c_int
     L.bgk_lattice_init.argtypes = [c_void_p, c_int, c_void_p, c_void_p]
     L.bgk_lattice_init.restype = c_int
     L.bgk_lattice_load.argtypes = [c_void_p, c_void_p, c_void_p]

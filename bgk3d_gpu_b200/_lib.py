@@ -84,6 +84,12 @@ def lib() -> ctypes.CDLL:
     L.bgk_draglift.argtypes = [P, POINTER(c_void_p), c_int, c_int, c_int, c_int, c_int, c_int,
                                c_void_p, c_void_p, c_size_t, c_void_p]
     L.bgk_draglift.restype = c_int
+    L.bgk_profile.argtypes = [P, POINTER(c_void_p), c_int, c_int, c_int, c_void_p, c_void_p]
+    L.bgk_profile.restype = c_int
+    L.bgk_probe.argtypes = [P, POINTER(c_void_p), c_int, c_int, c_int, c_void_p, c_void_p]
+    L.bgk_probe.restype = c_int
+    L.bgk_slice.argtypes = [P, POINTER(c_void_p), c_int, c_int, c_void_p, c_void_p]
+    L.bgk_slice.restype = c_int
     L.bgk_device_sync.argtypes = []
     L.bgk_device_sync.restype = c_int
     L.bgk_last_error.argtypes = []

@@ -28,7 +28,7 @@ NVCC_FLAGS = ARCH + [
     "-I" + INCLUDE, "-I" + CSRC,
 ]
 
-LIB_SOURCES = ["bgk_api.cu", "lattice.cu", "batch.cu", "noalloc.cu", "inst_f64.cu", "inst_f32.cu", "inst_f16.cu",
+LIB_SOURCES = ["bgk_api.cu", "lattice.cu", "lattice_io.cu", "diag.cu", "batch.cu", "noalloc.cu", "inst_f64.cu", "inst_f32.cu", "inst_f16.cu",
                "inst_bf16.cu", "inst_f32f64.cu"]
 LIB = "libbgk3d_b200.so"
 DROPIN_SP = "libbgk3d_dropin_sp.so"

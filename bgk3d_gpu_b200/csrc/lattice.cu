@@ -60,13 +60,6 @@ int aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
 }
 
 // AA: population p of the observable state lives in slot opp(p).
-void observable(const bgk_lattice* L, void** out) {
-    if (L->desc.pattern == BGK_PATTERN_AA)
-        for (int d = 0; d < 19; ++d) out[d] = L->a[opp_of(d)];
-    else
-        for (int d = 0; d < 19; ++d) out[d] = L->a[d];
-}
-
 // One time step on stream st (no graph); with mom, the FP64 partial moments
 // of the new state go to mom (one slot of 5 doubles per block).
 int one_step(bgk_lattice* L, cudaStream_t st, double* mom = nullptr) {
@@ -121,6 +114,33 @@ int ensure_workspace(const bgk_lattice* Lc) {
 }
 
 }  // namespace
+
+namespace bgk_lat {
+void observable(const bgk_lattice* L, void** out) {
+    if (L->desc.pattern == BGK_PATTERN_AA)
+        for (int d = 0; d < 19; ++d) out[d] = L->a[opp_of(d)];
+    else
+        for (int d = 0; d < 19; ++d) out[d] = L->a[d];
+}
+
+void begin_load(bgk_lattice* L, void** out) {
+    for (int q = 0; q < 19; ++q) L->a[q] = L->planes[q];
+    if (L->desc.pattern == BGK_PATTERN_AB) {
+        for (int q = 0; q < 18; ++q) L->b[q] = L->planes[19 + q];
+        L->b[18] = L->a[18];
+    }
+    observable(L, out);
+}
+
+int end_load(bgk_lattice* L, cudaStream_t st) {
+    L->steps = 0;
+    if (L->desc.pattern == BGK_PATTERN_AA && L->desc.bcase == BC_INFLOW)
+        if (int e = aa_prepass(&L->p, L->a, st)) return e;
+    return BGK_OK;
+}
+}  // namespace bgk_lat
+
+using bgk_lat::observable;
 
 extern "C" {
 
@@ -225,35 +245,23 @@ int bgk_lattice_load(bgk_lattice* L, const void* host, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const int l = L->desc.l, m = L->desc.m, n = L->desc.n;
     const size_t es = L->es, row = (size_t)(l + 2) * es, rows = (size_t)(m + 2) * (n + 2);
-    // AB: reset the pointer arrangement to the base planes
-    for (int q = 0; q < 19; ++q) L->a[q] = L->planes[q];
-    if (L->desc.pattern == BGK_PATTERN_AB) {
-        for (int q = 0; q < 18; ++q) L->b[q] = L->planes[19 + q];
-        L->b[18] = L->a[18];
-    }
+    void* f[19];
+    bgk_lat::begin_load(L, f);
     for (int d = 0; d < 19; ++d) {
-        void* dst = (L->desc.pattern == BGK_PATTERN_AA) ? L->a[opp_of(d)] : L->a[d];
+        void* dst = f[d];
         const char* src = (const char*)host + (size_t)d * row * rows;
         cudaError_t e = cudaMemcpy2DAsync(dst, (size_t)L->nx * es, src, row, row, rows, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "load: %s", cudaGetErrorString(e));
     }
-    L->steps = 0;
-    if (L->desc.pattern == BGK_PATTERN_AA && L->desc.bcase == BC_INFLOW)
-        if (int e = aa_prepass(&L->p, L->a, st)) return e;
-    return BGK_OK;
+    return bgk_lat::end_load(L, st);
 }
 
 int bgk_lattice_init(bgk_lattice* L, int flow, const double* params, void* stream) {
     if (!L) return set_error(BGK_ERR_ARG, "null lattice");
     if (flow < 0 || flow > 2) return set_error(BGK_ERR_ARG, "unknown flow %d", flow);
     cudaStream_t st = (cudaStream_t)stream;
-    for (int q = 0; q < 19; ++q) L->a[q] = L->planes[q];
-    if (L->desc.pattern == BGK_PATTERN_AB) {
-        for (int q = 0; q < 18; ++q) L->b[q] = L->planes[19 + q];
-        L->b[18] = L->a[18];
-    }
     void* f[19];
-    for (int d = 0; d < 19; ++d) f[d] = (L->desc.pattern == BGK_PATTERN_AA) ? L->a[opp_of(d)] : L->a[d];
+    bgk_lat::begin_load(L, f);
     const float scale = (L->desc.kind == K_F16 || L->desc.kind == K_BF16) ? L->desc.scale : 1.0f;
     int rc;
     {
@@ -267,10 +275,7 @@ int bgk_lattice_init(bgk_lattice* L, int flow, const double* params, void* strea
         }
     }
     if (rc) return rc;
-    L->steps = 0;
-    if (L->desc.pattern == BGK_PATTERN_AA && L->desc.bcase == BC_INFLOW)
-        if (int e = aa_prepass(&L->p, L->a, st)) return e;
-    return BGK_OK;
+    return bgk_lat::end_load(L, st);
 }
 
 int bgk_lattice_store(const bgk_lattice* L, void* host, void* stream) {

@@ -26,3 +26,14 @@ struct bgk_lattice {
     double* mom = nullptr;       // per-block partial moments of fused steps
     size_t mom_bytes = 0;
 };
+
+// Shared by the lattice's host-transfer paths (lattice.cu, lattice_io.cu).
+namespace bgk_lat {
+// Device arrays holding populations 01..19 of the observable state.
+void observable(const bgk_lattice* L, void** out);
+// Reset the pointer arrangement to the base planes and return the arrays a
+// new state of populations 01..19 is written to (AA: slot opp(d)).
+void begin_load(bgk_lattice* L, void** out);
+// After a new state is written: step count 0, AA outflow pre-pass.
+int end_load(bgk_lattice* L, cudaStream_t st);
+}  // namespace bgk_lat

@@ -9,6 +9,7 @@ SRC/draglift.F90) as FP64 device reductions.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -130,6 +131,29 @@ class DeviceLattice:
               "bgk_draglift")
         return self._out[:3].cpu().numpy().copy()
 
+    def _diag_call(self, fn, *args, n_out: int, dtype):
+        out = torch.empty(n_out, dtype=dtype, device=self.device)
+        a, _ = self._ptrs()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        check(getattr(lib(), fn)(ctypes.byref(self.params), a, *args, out.data_ptr(), st), fn)
+        return out.cpu().numpy()
+
+    def profile(self, axis: int, c1: int, c2: int) -> np.ndarray:
+        """(len, 5): position (t - 0.5), u_x, u_y, u_z, rho along a grid line (bgk_profile)."""
+        ln = (self.l, self.m, self.n)[axis] if axis in (0, 1, 2) else 1   # the library rejects bad axes
+        v = self._diag_call("bgk_profile", axis, c1, c2, n_out=4 * ln, dtype=torch.float64).reshape(ln, 4)
+        return np.column_stack([np.arange(1, ln + 1) - 0.5, v])
+
+    def probe(self, i: int, j: int, k: int) -> np.ndarray:
+        """(u_x, u_y, u_z, rho) at one node (bgk_probe)."""
+        return self._diag_call("bgk_probe", i, j, k, n_out=4, dtype=torch.float64)
+
+    def slice(self, plane: int, index: int) -> np.ndarray:
+        """(n2, n1, 3) float32 velocity over a plane (bgk_slice)."""
+        n1 = self.m if plane == 2 else self.l
+        n2 = self.m if plane == 0 else self.n    # (the library rejects planes other than 0, 1, 2)
+        return self._diag_call("bgk_slice", plane, index, n_out=3 * n1 * n2, dtype=torch.float32).reshape(n2, n1, 3)
+
 
 class Lattice:
     """A library-owned lattice (bgk_lattice_*): padded aligned layout, AB or
@@ -193,6 +217,45 @@ class Lattice:
         """Equilibrium state of an analytic flow computed on the device."""
         arr = (ctypes.c_double * 4)(*([float(v) for v in params] + [0.0] * (4 - len(params))))
         check(self.L.bgk_lattice_init(self.h, self.FLOWS[flow], arr, self._stream()), "bgk_lattice_init")
+
+    def profile(self, axis: int, c1: int, c2: int) -> np.ndarray:
+        """(len, 5): position (t - 0.5), u_x, u_y, u_z, rho along a grid line
+        (bgk_lattice_profile; axis 0 = prof_i at (j, k) = (c1, c2), 1 = prof_j
+        at (i, k), 2 = prof_k at (i, j))."""
+        ln = (self.l, self.m, self.n)[axis] if axis in (0, 1, 2) else 1   # the library rejects bad axes
+        out = torch.empty(4 * ln, dtype=torch.float64, device=self.device)
+        check(self.L.bgk_lattice_profile(self.h, axis, c1, c2, out.data_ptr(), self._stream()),
+              "bgk_lattice_profile")
+        return np.column_stack([np.arange(1, ln + 1) - 0.5, out.cpu().numpy().reshape(ln, 4)])
+
+    def probe(self, i: int, j: int, k: int) -> np.ndarray:
+        """(u_x, u_y, u_z, rho) at one node (bgk_lattice_probe)."""
+        out = torch.empty(4, dtype=torch.float64, device=self.device)
+        check(self.L.bgk_lattice_probe(self.h, i, j, k, out.data_ptr(), self._stream()), "bgk_lattice_probe")
+        return out.cpu().numpy()
+
+    def slice(self, plane: int, index: int) -> np.ndarray:
+        """(n2, n1, 3) float32 velocity over a plane (bgk_lattice_slice; plane 0
+        = xy at k = index, 1 = xz at j = index, 2 = yz at i = index)."""
+        n1 = self.m if plane == 2 else self.l
+        n2 = self.m if plane == 0 else self.n    # (the library rejects planes other than 0, 1, 2)
+        out = torch.empty(3 * n1 * n2, dtype=torch.float32, device=self.device)
+        check(self.L.bgk_lattice_slice(self.h, plane, index, out.data_ptr(), self._stream()), "bgk_lattice_slice")
+        return out.cpu().numpy().reshape(n2, n1, 3)
+
+    def save(self, path, itime: int | None = None, file_bytes: int = 0) -> None:
+        """Restart file in the reference's record format (bgk_lattice_save);
+        itime defaults to the lattice's step count."""
+        it = self.steps if itime is None else int(itime)
+        check(self.L.bgk_lattice_save(self.h, os.fsencode(path), it, int(file_bytes), self._stream()),
+              "bgk_lattice_save")
+
+    def restore(self, path) -> int:
+        """Load a restart file (bgk_lattice_restore); returns its time step."""
+        it = ctypes.c_int(0)
+        check(self.L.bgk_lattice_restore(self.h, os.fsencode(path), ctypes.byref(it), self._stream()),
+              "bgk_lattice_restore")
+        return int(it.value)
 
     def download(self) -> np.ndarray:
         dt = {0: np.float64, 1: np.float32, 2: np.uint16, 3: np.uint16, 4: np.float32}[self.kind]
@@ -279,3 +342,8 @@ class Batch:
     @property
     def nodes(self) -> int:
         return int(self.L.bgk_batch_nodes(self.h))
+
+
+def save_name(itime: int) -> str:
+    """The reference's restart file name for a time step (SRC/save_raw.F90:39-41)."""
+    return f"save.{int(itime):08d}.bin"

@@ -15,6 +15,10 @@
  *   bgk_moments    <- diagno            SRC/diagno.F90:87-138 (host/OpenACC
  *                                       reduction in the reference)
  *   bgk_draglift   <- draglift          SRC/draglift.F90:77-181
+ *   bgk_profile    <- prof_i/_j/_k      SRC/prof_k.F90:47-87 (host loops
+ *                                       after a full-state copy in the reference)
+ *   bgk_probe      <- probe             SRC/probe.F90:50-78
+ *   bgk_slice      <- vtk_xy/xz/yz_bin  SRC/vtk_xy.binary.F90:78-97
  *   bgk_device_sync<- gpu_device_sync   SRC/bcond_gpu.hpp:548-571
  * The reference-named drop-in symbols themselves are declared in
  * bgk3d_dropin.h.
@@ -120,6 +124,27 @@ size_t bgk_moments_noalloc_max_bytes(void);
    (SRC/draglift.F90:77-176) into out_dev[0..2]. */
 int bgk_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
                  int ke, double* out_dev, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Velocity and density along a grid line, computed on the device with the
+   arithmetic of SRC/prof_k.F90:47-77 (prof_i, prof_j likewise): density =
+   sum of the 19 stored values (storage arithmetic) + cte1 (1, compute type),
+   velocity = momentum sum (storage arithmetic) / density (compute type).
+   axis 0 runs i = 1..l at (j, k) = (c1, c2) (prof_i), 1 runs j = 1..m at
+   (i, k) = (c1, c2) (prof_j), 2 runs k = 1..n at (i, j) = (c1, c2) (prof_k).
+   out_dev: 4 doubles per node (u_x, u_y, u_z, rho); the reference writes
+   them as (position, u_x, u_y, u_z, rho) with u_y its "w" and u_z its "v". */
+int bgk_profile(const bgk_sweep_params* p, void* const* a, int axis, int c1, int c2, double* out_dev,
+                void* stream);
+
+/* Velocity and density at node (i, j, k) with the arithmetic of
+   SRC/probe.F90:50-78 (all in the compute type): out_dev = (u_x, u_y, u_z, rho). */
+int bgk_probe(const bgk_sweep_params* p, void* const* a, int i, int j, int k, double* out_dev, void* stream);
+
+/* Velocity over a plane in single precision, SRC/vtk_xy.binary.F90:78-97:
+   plane 0 = xy at k = index (out[j][i]), 1 = xz at j = index (out[k][i]),
+   2 = yz at i = index (out[k][j]); 3 floats (u_x, u_y, u_z) per node, the
+   order the reference's VTK writers emit. */
+int bgk_slice(const bgk_sweep_params* p, void* const* a, int plane, int index, float* out_dev, void* stream);
 
 /* Helpers of the drop-in library's tracked moments (bgk3d_dropin.h):
    bgk_sweep with per-block partial moments into partials (when they fit;

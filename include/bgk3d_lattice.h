@@ -68,6 +68,34 @@ int bgk_lattice_store(const bgk_lattice* lat, void* host, void* stream);
    step count like bgk_lattice_load. */
 int bgk_lattice_init(bgk_lattice* lat, int flow, const double* params, void* stream);
 
+/* Restart files in the reference's record format (SRC/save_raw.F90:37-69,
+   SRC/restore_raw.F90:35-61): a Fortran sequential unformatted file of 20
+   records framed by 4-byte length markers -- the time step (4-byte
+   integer), then populations 01..19 over the full halo box (0..l+1, 0..m+1,
+   0..n+1), i fastest.  Records over 2147483639 bytes are split into
+   subrecords the gfortran way (negative leading marker: more follows;
+   negative trailing marker: continues an earlier subrecord).
+   save: file_bytes 0 writes the stored elements as they are (16-bit kinds:
+   the scaled 16-bit patterns); 4 or 8 converts on the device to real*4 /
+   real*8 (16-bit kinds unscaled), what a reference build of that precision
+   restores.  AA lattices must be at an even step.  The file name is the
+   caller's (the reference writes save.<itime, 8 digits>.bin and restores
+   from restore.bin).
+   restore: the element size is taken from the record lengths; 2-byte values
+   go as they are into a 16-bit lattice and are read as IEEE half values into
+   a 4- or 8-byte one (the reference's HALF storage); other sizes are
+   converted on the device.  The file's box must be this lattice's; the
+   framing of all records is checked before the lattice is touched.  Sets
+   *itime (if not null) to the file's time step and resets the step count
+   like bgk_lattice_load.  Both return after the data is written/read. */
+int bgk_lattice_save(const bgk_lattice* lat, const char* path, int itime, int file_bytes, void* stream);
+int bgk_lattice_restore(bgk_lattice* lat, const char* path, int* itime, void* stream);
+/* Largest subrecord bgk_lattice_save writes (default and maximum 2147483639
+   bytes; values outside 4..2147483639 are ignored); returns the previous
+   limit.  Lowering it exercises the subrecord framing with small lattices.
+   No counterpart in the reference. */
+long long bgk_io_set_subrecord_limit(long long bytes);
+
 /* Advance nsteps time steps (boundaries + stream + collide), stream-ordered.
    Runs of 16 or more steps replay a captured CUDA graph. */
 int bgk_lattice_step(bgk_lattice* lat, int nsteps, void* stream);
@@ -87,6 +115,12 @@ int bgk_lattice_moments(const bgk_lattice* lat, double* out_dev, void* stream);
 /* FP64 drag/lift (as bgk_draglift) over the box into out_dev[0..2]. */
 int bgk_lattice_draglift(const bgk_lattice* lat, int is, int ie, int js, int je, int ks, int ke,
                          double* out_dev, void* stream);
+
+/* bgk_profile / bgk_probe / bgk_slice on the lattice's current state (AA
+   lattices: at an even step). */
+int bgk_lattice_profile(const bgk_lattice* lat, int axis, int c1, int c2, double* out_dev, void* stream);
+int bgk_lattice_probe(const bgk_lattice* lat, int i, int j, int k, double* out_dev, void* stream);
+int bgk_lattice_slice(const bgk_lattice* lat, int plane, int index, float* out_dev, void* stream);
 
 /* Steps advanced since the last load. */
 long long bgk_lattice_steps(const bgk_lattice* lat);

@@ -578,6 +578,77 @@ void draglift(Ctx<S, C>& A, const int32_t* obs, int l, int m, int n, int is, int
     out[0] = F[0]; out[1] = F[1]; out[2] = F[2];
 }
 
+// ------------------------------------------------- profiles, probe, slices
+// The storage arithmetic: the reference sums the storage arrays directly in
+// these routines, so the arithmetic is the storage kind's (float for the
+// 4-byte and, here, the 16-bit kinds, whose values are unscaled first).
+template <class S> struct ArithOf { typedef float type; };
+template <> struct ArithOf<double> { typedef double type; };
+
+// SRC/prof_k.F90:47-77 (SRC/prof_i.F90:48-77, SRC/prof_j.F90:48-77 likewise):
+// den = a01+...+a19 (storage arithmetic) + cte1 (compute type), u = (x
+// momentum sum, storage arithmetic) / den in the compute type.  axis 0 runs
+// i at (j, k) = (c1, c2), axis 1 runs j at (i, k) = (c1, c2), axis 2 runs k
+// at (i, j) = (c1, c2).  out: 4 values per node (u_x, u_y, u_z, rho).
+template <class S, class C>
+void profile(Ctx<S, C>& A, int axis, int c1, int c2, int len, C cte1, double* out) {
+    typedef typename ArithOf<S>::type R;
+    for (int t = 1; t <= len; ++t) {
+        const int i = axis == 0 ? t : c1, j = axis == 1 ? t : (axis == 0 ? c1 : c2), k = axis == 2 ? t : c2;
+        R x[19];
+        for (int p = 0; p < 19; ++p) x[p] = (R)A.ld(p + 1, i, j, k);
+        const R s = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] + x[11] +
+                    x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18];
+        const C den = (C)s + cte1;
+        const R sx = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
+        const R sy = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
+        const R sz = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
+        double* o = out + 4 * (long)(t - 1);
+        o[0] = (double)((C)sx / den); o[1] = (double)((C)sy / den); o[2] = (double)((C)sz / den);
+        o[3] = (double)den;
+    }
+}
+
+// SRC/probe.F90:50-78: populations copied into compute-type variables first,
+// rho and the momentum summed in the compute type.  out = (u_x, u_y, u_z, rho).
+template <class S, class C>
+void probe(Ctx<S, C>& A, int i, int j, int k, C cte1, double* out) {
+    C x[19];
+    for (int p = 0; p < 19; ++p) x[p] = A.ld(p + 1, i, j, k);
+    const C rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] + x[11] + x[12] +
+                  x[13] + x[14] + x[15] + x[16] + x[17] + x[18] + cte1;
+    const C xj = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
+    const C yj = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
+    const C zj = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
+    out[0] = (double)(xj / rho); out[1] = (double)(yj / rho); out[2] = (double)(zj / rho); out[3] = (double)rho;
+}
+
+// SRC/vtk_xy.binary.F90:78-97 (vtk_xz / vtk_yz likewise): u, den in single
+// precision -- each sum in the storage arithmetic (den with cte1 = 1.0),
+// rounded to float -- and u/den in float.  plane 0: xy at k = index (j, i
+// loops), 1: xz at j = index (k, i), 2: yz at i = index (k, j); out: 3
+// floats per node, inner index fastest.
+template <class S, class C>
+void slice(Ctx<S, C>& A, int plane, int index, int l, int m, int n, float* out) {
+    typedef typename ArithOf<S>::type R;
+    const int n1 = plane == 2 ? m : l, n2 = plane == 0 ? m : n;
+    long o = 0;
+    for (int b = 1; b <= n2; ++b)
+        for (int a = 1; a <= n1; ++a) {
+            const int i = plane == 2 ? index : a;
+            const int j = plane == 0 ? b : (plane == 1 ? index : a);
+            const int k = plane == 0 ? index : b;
+            R x[19];
+            for (int p = 0; p < 19; ++p) x[p] = (R)A.ld(p + 1, i, j, k);
+            const float u = (float)(x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]);
+            const float w = (float)(x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]);
+            const float v = (float)(x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]);
+            const float den = (float)(x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] +
+                                      x[11] + x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18] + (R)1.0);
+            out[o++] = u / den; out[o++] = w / den; out[o++] = v / den;
+        }
+}
+
 template <class S, class C>
 void make(Ctx<S, C>& c, void** a, int nx, int ny, const float* scale) {
     make_ctx_common(c, a, nx, ny, scale);
@@ -649,6 +720,34 @@ int orc_draglift(int kind, void** a, const int32_t* obs, int l, int m, int n, in
     DISPATCH(kind, {
         Ctx<S, C> A; make(A, a, nx, ny, scale);
         draglift(A, obs, l, m, n, is, ie, js, je, ks, ke, out);
+    });
+    return 0;
+}
+
+int orc_profile(int kind, void** a, int l, int m, int n, int nx, int ny, int axis, int c1, int c2,
+                double cte1, const float* scale, double* out) {
+    const int len = axis == 0 ? l : (axis == 1 ? m : n);
+    DISPATCH(kind, {
+        Ctx<S, C> A; make(A, a, nx, ny, scale);
+        profile(A, axis, c1, c2, len, (C)cte1, out);
+    });
+    return 0;
+}
+
+int orc_probe(int kind, void** a, int nx, int ny, int i, int j, int k, double cte1, const float* scale,
+              double* out) {
+    DISPATCH(kind, {
+        Ctx<S, C> A; make(A, a, nx, ny, scale);
+        probe(A, i, j, k, (C)cte1, out);
+    });
+    return 0;
+}
+
+int orc_slice(int kind, void** a, int l, int m, int n, int nx, int ny, int plane, int index,
+              const float* scale, float* out) {
+    DISPATCH(kind, {
+        Ctx<S, C> A; make(A, a, nx, ny, scale);
+        slice(A, plane, index, l, m, n, out);
     });
     return 0;
 }

@@ -52,6 +52,9 @@ def lib() -> ctypes.CDLL:
         L.orc_diagno.argtypes = [c_int, pp, c_int, c_int, c_int, c_int, c_int, c_void_p, c_double,
                                  fp, dp]
         L.orc_draglift.argtypes = [c_int, pp, c_void_p] + [c_int] * 11 + [fp, dp]
+        L.orc_profile.argtypes = [c_int, pp] + [c_int] * 8 + [c_double, fp, dp]
+        L.orc_probe.argtypes = [c_int, pp] + [c_int] * 5 + [c_double, fp, dp]
+        L.orc_slice.argtypes = [c_int, pp] + [c_int] * 7 + [fp, fp]
         L.orc_float_to_half.argtypes = [c_float]
         L.orc_float_to_half.restype = ctypes.c_uint16
         L.orc_half_to_float.argtypes = [ctypes.c_uint16]
@@ -162,6 +165,33 @@ class OracleLattice:
                                 self.n, self.nx, self.ny, *box, self.scale, out)
         assert rc == 0
         return np.array(out[:])
+
+    def profile(self, axis: int, c1: int, c2: int, cte1: float = 1.0) -> np.ndarray:
+        """(len, 4) (u_x, u_y, u_z, rho) along a grid line (SRC/prof_k.F90:47-77)."""
+        ln = (self.l, self.m, self.n)[axis]
+        out = np.zeros((ln, 4))
+        rc = lib().orc_profile(self.kind, _ptrs(self.a), self.l, self.m, self.n, self.nx, self.ny, axis, c1, c2,
+                               cte1, self.scale, out.ctypes.data_as(POINTER(c_double)))
+        assert rc == 0
+        return out
+
+    def probe(self, i: int, j: int, k: int, cte1: float = 1.0) -> np.ndarray:
+        """(u_x, u_y, u_z, rho) at one node (SRC/probe.F90:50-78)."""
+        out = np.zeros(4)
+        rc = lib().orc_probe(self.kind, _ptrs(self.a), self.nx, self.ny, i, j, k, cte1, self.scale,
+                             out.ctypes.data_as(POINTER(c_double)))
+        assert rc == 0
+        return out
+
+    def slice(self, plane: int, index: int) -> np.ndarray:
+        """(n2, n1, 3) float32 velocity of a VTK slice (SRC/vtk_xy.binary.F90:78-97)."""
+        n1 = self.m if plane == 2 else self.l
+        n2 = self.m if plane == 0 else self.n
+        out = np.zeros((n2, n1, 3), np.float32)
+        rc = lib().orc_slice(self.kind, _ptrs(self.a), self.l, self.m, self.n, self.nx, self.ny, plane, index,
+                             self.scale, out.ctypes.data_as(POINTER(c_float)))
+        assert rc == 0
+        return out
 
     def fluid_mask(self) -> np.ndarray:
         """(n, m, l) bool mask of the nodes whose values are defined."""
