@@ -15,6 +15,7 @@ class LatticeDesc(Structure):
         ("force_mode", c_int), ("fx", c_double), ("fy", c_double), ("fz", c_double),
         ("lid_force", c_double), ("u_inflow", c_double),
         ("scale", c_float),
+        ("fast", c_int),
     ]
 
 

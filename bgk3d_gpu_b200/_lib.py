@@ -44,6 +44,7 @@ class SweepParams(Structure):
         ("obs", c_void_p), ("obs_nx", c_int), ("obs_ny", c_int),
         ("imin", c_int), ("imax", c_int), ("jmin", c_int), ("jmax", c_int),
         ("kmin", c_int), ("kmax", c_int),
+        ("fast", c_int),
     ]
 
 

@@ -28,8 +28,8 @@ NVCC_FLAGS = ARCH + [
     "-I" + INCLUDE, "-I" + CSRC,
 ]
 
-LIB_SOURCES = ["bgk_api.cu", "lattice.cu", "lattice_io.cu", "diag.cu", "batch.cu", "noalloc.cu", "inst_f64.cu", "inst_f32.cu", "inst_f16.cu",
-               "inst_bf16.cu", "inst_f32f64.cu"]
+LIB_SOURCES = ["bgk_api.cu", "lattice.cu", "lattice_io.cu", "diag.cu", "batch.cu", "noalloc.cu"] + [
+    f"inst_{kind}_{group}.cu" for kind in ("f64", "f32", "f16", "bf16", "f32f64") for group in ("ab", "aa", "batch", "misc")]
 LIB = "libbgk3d_b200.so"
 DROPIN_SP = "libbgk3d_dropin_sp.so"
 DROPIN_DP = "libbgk3d_dropin_dp.so"

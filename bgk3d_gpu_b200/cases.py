@@ -131,10 +131,11 @@ def sphere(l: int = 512, m: int = 256, n: int = 256, kind: str = "f32", diameter
 
 
 LATTICE_KEYS = ("kind", "bcase", "omega", "lid_force", "u_inflow", "force_mode", "force", "scale",
-                "pattern")
+                "pattern", "fast")
 
 
-def make_lattice(case: dict, pattern: str = "ab", scale: float | None = None, on_device: bool = True):
+def make_lattice(case: dict, pattern: str = "ab", scale: float | None = None, on_device: bool = True,
+                 fast: bool | None = None):
     """Create a Lattice for the case, set its obstacle and its initial state:
     computed on the device for the analytic flows (default), else built with
     torch and loaded from the host."""
@@ -142,6 +143,8 @@ def make_lattice(case: dict, pattern: str = "ab", scale: float | None = None, on
     from .lattice import Lattice
     kw = {k: case[k] for k in LATTICE_KEYS if k in case}
     kw["pattern"] = pattern
+    if fast is not None:
+        kw["fast"] = fast
     if scale is not None:
         kw["scale"] = scale
     elif kw.get("kind") == "f16":

@@ -25,27 +25,31 @@ template <class S, class C> struct BatchView {
     int sub;                       // tiles taken per queue access
 };
 
+// One node of the tile's lattice: boundary case and collision mode chosen at
+// run time (the obstacle test is always compiled in, P.obs decides).
+template <class S, class C, int BC>
+__device__ __forceinline__ void batch_node_bc(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
+    const int cm = P.generic + (sizeof(C) == 4 ? 2 * P.fast : 0);
+    switch (cm) {
+        case CM_STRICT: sweep_node<S, C, BC, int, CM_STRICT, true>(P, gw, m5); break;
+        case CM_STRICT_GENERIC: sweep_node<S, C, BC, int, CM_STRICT_GENERIC, true>(P, gw, m5); break;
+        case CM_FAST:
+            if constexpr (sizeof(C) == 4) sweep_node<S, C, BC, int, CM_FAST, true>(P, gw, m5);
+            break;
+        default:
+            if constexpr (sizeof(C) == 4) sweep_node<S, C, BC, int, CM_FAST_GENERIC, true>(P, gw, m5);
+            break;
+    }
+}
+
 template <class S, class C>
 __device__ __forceinline__ void batch_node(const SweepArgs<S, C>& P, uint32_t gw) {
     double m5[5];
-    const bool g = P.generic != 0;
     switch (P.bcase) {
-        case BC_DRIVEN:
-            if (g) sweep_node<S, C, BC_DRIVEN, int, true>(P, gw, m5);
-            else sweep_node<S, C, BC_DRIVEN, int, false>(P, gw, m5);
-            break;
-        case BC_PERIODIC:
-            if (g) sweep_node<S, C, BC_PERIODIC, int, true>(P, gw, m5);
-            else sweep_node<S, C, BC_PERIODIC, int, false>(P, gw, m5);
-            break;
-        case BC_CHANNEL:
-            if (g) sweep_node<S, C, BC_CHANNEL, int, true>(P, gw, m5);
-            else sweep_node<S, C, BC_CHANNEL, int, false>(P, gw, m5);
-            break;
-        case BC_INFLOW:
-            if (g) sweep_node<S, C, BC_INFLOW, int, true>(P, gw, m5);
-            else sweep_node<S, C, BC_INFLOW, int, false>(P, gw, m5);
-            break;
+        case BC_DRIVEN: batch_node_bc<S, C, BC_DRIVEN>(P, gw, m5); break;
+        case BC_PERIODIC: batch_node_bc<S, C, BC_PERIODIC>(P, gw, m5); break;
+        case BC_CHANNEL: batch_node_bc<S, C, BC_CHANNEL>(P, gw, m5); break;
+        case BC_INFLOW: batch_node_bc<S, C, BC_INFLOW>(P, gw, m5); break;
         default: break;
     }
 }

@@ -1,6 +1,7 @@
 // Host-side construction of kernel arguments, shared by the library's
 // translation units (typed ABI and library-owned lattices).
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include "bgk3d_b200.h"
 #include "sweep_ab.cuh"
@@ -8,15 +9,59 @@
 
 namespace bgk {
 
+// Storage scale of the 16-bit kinds (1 otherwise).
+inline double storage_scale(const bgk_sweep_params* p) {
+    return (p->kind == K_F16 || p->kind == K_BF16) ? (double)p->scale : 1.0;
+}
+
+// Collision constants in the compute type; with sc != 1 the weights and the
+// forces are in storage units.  Each constant is rounded to C first and then
+// scaled (exact for power-of-two scales), so the products equal the
+// physical constants times the scale.
 template <class C>
-ColConst<C> col_const(const bgk_sweep_params* p) {
+ColConst<C> col_const(const bgk_sweep_params* p, double sc = 1.0) {
     ColConst<C> k;
     k.omega = (C)p->omega; k.cte0 = (C)p->cte0; k.cte1 = (C)p->cte1;
-    k.p0 = (C)p->p0; k.p1 = (C)p->p1; k.p2 = (C)p->p2;
+    k.p0 = (C)p->p0 * (C)sc; k.p1 = (C)p->p1 * (C)sc; k.p2 = (C)p->p2 * (C)sc;
     k.rf = (C)p->rf; k.qf = (C)p->qf; k.tre = (C)p->tre;
     k.force_mode = p->force_mode;
-    k.fx = (C)p->fx; k.fy = (C)p->fy; k.fz = (C)p->fz;
+    k.fx = (C)p->fx * (C)sc; k.fy = (C)p->fy * (C)sc; k.fz = (C)p->fz * (C)sc;
     return k;
+}
+
+// v rounded to `bits` significant bits.
+inline double round_to_bits(double v, int bits) {
+    int e;
+    const double m = std::frexp(v, &e);
+    return std::ldexp(std::nearbyint(std::ldexp(m, bits)), e - bits);
+}
+
+// Constants of the fused-multiply-add collision (d3q19.cuh), in storage units.
+// Momentum is conserved only if (1 - omega) + (2 r1 + 8 r2) = 1 in the
+// arithmetic that runs: rounded independently, the two parts miss 1 by a few
+// 1e-8, and the momentum drifts by that factor every step (measured: 4e-5
+// kinetic-energy error after 400 steps).  So r2 is rounded to two bits fewer
+// than C holds, r1 = 2 r2 (p1 = 2 p2), 2 r1 + 8 r2 = 12 r2 and 1 - 12 r2 are
+// then exact in C, and the other constants use that omega' = 12 r2 / rf / 3.
+template <class C>
+FastConst<C> fast_const(const bgk_sweep_params* p, double sc) {
+    FastConst<C> f;
+    const int bits = sizeof(C) == 4 ? 22 : 51;
+    const double k2 = round_to_bits(p->omega * p->rf * p->p2, bits);
+    const double k1 = (p->p1 == 2.0 * p->p2) ? 2.0 * k2 : round_to_bits(p->omega * p->rf * p->p1, bits);
+    const double om = 2.0 * k1 + 8.0 * k2;   // omega' (= omega (1 + O(1e-7)) for the reference weights)
+    f.omc = (C)(1.0 - om);
+    f.r1 = (C)(k1 * sc);
+    f.r2 = (C)(k2 * sc);
+    f.a1 = (C)(om * p->qf * p->tre * p->p1 * sc);
+    f.a2 = (C)(om * p->qf * p->tre * p->p2 * sc);
+    f.b0 = (C)(om * p->p0 * sc);
+    f.b1 = (C)(om * p->p1 * sc);
+    f.b2 = (C)(om * p->p2 * sc);
+    f.qf = (C)p->qf; f.cte0 = (C)p->cte0; f.cte1 = (C)p->cte1;
+    f.force_mode = p->force_mode;
+    f.fx = (C)(p->fx * sc); f.fy = (C)(p->fy * sc); f.fz = (C)(p->fz * sc);
+    return f;
 }
 
 template <class S, class C>
@@ -28,8 +73,10 @@ SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* cons
     }
     A.nx = p->nx; A.nxy = p->nx * p->ny;
     A.l = p->l; A.m = p->m; A.n = p->n;
-    A.col = col_const<C>(p);
-    A.lid_force = (C)p->lid_force;
+    const double sc = storage_scale(p);
+    A.col = col_const<C>(p, sc);
+    A.fc = fast_const<C>(p, sc);
+    A.lid_force = (C)p->lid_force * (C)sc;
     A.u_inflow = (C)p->u_inflow;
     A.inflow_cte1 = (C)p->inflow_cte1;
     A.scale = (p->kind == K_F16 || p->kind == K_BF16) ? p->scale : 1.0f;
@@ -42,6 +89,7 @@ SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* cons
     A.mom = nullptr;
     A.bcase = p->bcase;
     A.generic = !(p->cte1 == 1.0 && p->cte0 == 0.0 && p->fx == 0.0 && p->fy == 0.0 && p->fz == 0.0);
+    A.fast = (p->fast != 0 && sizeof(C) == 4) ? 1 : 0;
     return A;
 }
 

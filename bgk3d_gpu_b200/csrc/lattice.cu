@@ -173,6 +173,7 @@ int bgk_lattice_create(const bgk_lattice_desc* d, bgk_lattice** out) {
     L->p.force_mode = d->force_mode; L->p.fx = d->fx; L->p.fy = d->fy; L->p.fz = d->fz;
     L->p.lid_force = d->lid_force; L->p.u_inflow = d->u_inflow; L->p.inflow_cte1 = 0.0;
     L->p.scale = d->scale;
+    L->p.fast = d->fast;
     if (int e = validate(&L->p)) { delete L; return e; }
     L->bytes = bgk_lattice_device_bytes(d);
     cudaError_t e = cudaMalloc(&L->base, L->bytes);

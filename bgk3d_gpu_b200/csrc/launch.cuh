@@ -13,16 +13,63 @@
 
 namespace bgk {
 
-template <class S, class C, int BC>
-void launch_sweep_bc(const SweepArgs<S, C>& A, long long nelem, unsigned blocks, bool generic,
-                     cudaStream_t st) {
-    if (nelem < (1LL << 31)) {
-        if (generic) sweep_ab_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
-        else sweep_ab_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
-    } else {
-        if (generic) sweep_ab_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
-        else sweep_ab_kernel<S, C, BC, long long, false><<<blocks, 256, 0, st>>>(A);
+// Kernel variants: collision mode CM (fused-multiply-add modes for float
+// compute only) and obstacle logic OBS, for 32-bit offsets; lattices of 2^31
+// elements or more take 64-bit offsets with the generic collision and the
+// obstacle logic compiled in.
+template <template <class, class, int, class, int, bool> class L, class S, class C, int BC, class... A>
+void by_variant(long long nelem, int cm, bool obs, A... args) {
+    constexpr bool FLOAT = sizeof(C) == 4;
+    if (nelem >= (1LL << 31)) {
+        if constexpr (FLOAT) {
+            if (cm_fast(cm)) { L<S, C, BC, long long, CM_FAST_GENERIC, true>::go(args...); return; }
+        }
+        L<S, C, BC, long long, CM_STRICT_GENERIC, true>::go(args...);
+        return;
     }
+    switch (cm) {
+        case CM_STRICT:
+            if (obs) L<S, C, BC, int, CM_STRICT, true>::go(args...);
+            else L<S, C, BC, int, CM_STRICT, false>::go(args...);
+            break;
+        case CM_STRICT_GENERIC:
+            if (obs) L<S, C, BC, int, CM_STRICT_GENERIC, true>::go(args...);
+            else L<S, C, BC, int, CM_STRICT_GENERIC, false>::go(args...);
+            break;
+        case CM_FAST:
+            if constexpr (FLOAT) {
+                if (obs) L<S, C, BC, int, CM_FAST, true>::go(args...);
+                else L<S, C, BC, int, CM_FAST, false>::go(args...);
+            }
+            break;
+        default:
+            if constexpr (FLOAT) {
+                if (obs) L<S, C, BC, int, CM_FAST_GENERIC, true>::go(args...);
+                else L<S, C, BC, int, CM_FAST_GENERIC, false>::go(args...);
+            }
+            break;
+    }
+}
+
+template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbLaunch {
+    static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
+        sweep_ab_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
+    }
+};
+template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AaEvenLaunch {
+    static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
+        aa_even_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
+    }
+};
+template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AaOddLaunch {
+    static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
+        aa_odd_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
+    }
+};
+
+// Collision mode of the arguments (fast modes need float compute).
+template <class S, class C> int coll_mode(const SweepArgs<S, C>& A) {
+    return A.generic + ((sizeof(C) == 4 && A.fast) ? 2 : 0);
 }
 
 template <class S, class C>
@@ -39,14 +86,15 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     const long long blocks = (warps + 7) / 8;
     if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
-    const bool g = generic_collision(p);
+    const int cm = coll_mode(A);
+    const bool obs = A.obs != nullptr;
     const unsigned nb = (unsigned)blocks;
     switch (p->bcase) {
-        case BC_NONE: launch_sweep_bc<S, C, BC_NONE>(A, nelem, nb, g, st); break;
-        case BC_DRIVEN: launch_sweep_bc<S, C, BC_DRIVEN>(A, nelem, nb, g, st); break;
-        case BC_PERIODIC: launch_sweep_bc<S, C, BC_PERIODIC>(A, nelem, nb, g, st); break;
-        case BC_CHANNEL: launch_sweep_bc<S, C, BC_CHANNEL>(A, nelem, nb, g, st); break;
-        case BC_INFLOW: launch_sweep_bc<S, C, BC_INFLOW>(A, nelem, nb, g, st); break;
+        case BC_NONE: by_variant<AbLaunch, S, C, BC_NONE>(nelem, cm, obs, A, nb, st); break;
+        case BC_DRIVEN: by_variant<AbLaunch, S, C, BC_DRIVEN>(nelem, cm, obs, A, nb, st); break;
+        case BC_PERIODIC: by_variant<AbLaunch, S, C, BC_PERIODIC>(nelem, cm, obs, A, nb, st); break;
+        case BC_CHANNEL: by_variant<AbLaunch, S, C, BC_CHANNEL>(nelem, cm, obs, A, nb, st); break;
+        case BC_INFLOW: by_variant<AbLaunch, S, C, BC_INFLOW>(nelem, cm, obs, A, nb, st); break;
     }
     return check_launch("sweep_ab_kernel");
 }
@@ -79,20 +127,11 @@ int launch_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, i
 }
 
 template <class S, class C, int BC>
-void launch_aa_bc(const SweepArgs<S, C>& A, bool odd, bool generic, long long nelem, unsigned blocks,
-                  cudaStream_t st) {
-    if (nelem < (1LL << 31)) {
-        if (odd) {
-            if (generic) aa_odd_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
-            else aa_odd_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
-        } else {
-            if (generic) aa_even_kernel<S, C, BC, int, true><<<blocks, 256, 0, st>>>(A);
-            else aa_even_kernel<S, C, BC, int, false><<<blocks, 256, 0, st>>>(A);
-        }
-    } else {
-        if (odd) aa_odd_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
-        else aa_even_kernel<S, C, BC, long long, true><<<blocks, 256, 0, st>>>(A);
-    }
+void launch_aa_bc(const SweepArgs<S, C>& A, bool odd, long long nelem, unsigned blocks, cudaStream_t st) {
+    const int cm = coll_mode(A);
+    const bool obs = A.obs != nullptr;
+    if (odd) by_variant<AaOddLaunch, S, C, BC>(nelem, cm, obs, A, blocks, st);
+    else by_variant<AaEvenLaunch, S, C, BC>(nelem, cm, obs, A, blocks, st);
 }
 
 template <class S, class C>
@@ -105,12 +144,11 @@ int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* m
     if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
     const unsigned blocks = (unsigned)((warps + 7) / 8);
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
-    const bool g = generic_collision(p);
     switch (p->bcase) {
-        case BC_DRIVEN: launch_aa_bc<S, C, BC_DRIVEN>(A, odd, g, nelem, blocks, st); break;
-        case BC_PERIODIC: launch_aa_bc<S, C, BC_PERIODIC>(A, odd, g, nelem, blocks, st); break;
-        case BC_CHANNEL: launch_aa_bc<S, C, BC_CHANNEL>(A, odd, g, nelem, blocks, st); break;
-        case BC_INFLOW: launch_aa_bc<S, C, BC_INFLOW>(A, odd, g, nelem, blocks, st); break;
+        case BC_DRIVEN: launch_aa_bc<S, C, BC_DRIVEN>(A, odd, nelem, blocks, st); break;
+        case BC_PERIODIC: launch_aa_bc<S, C, BC_PERIODIC>(A, odd, nelem, blocks, st); break;
+        case BC_CHANNEL: launch_aa_bc<S, C, BC_CHANNEL>(A, odd, nelem, blocks, st); break;
+        case BC_INFLOW: launch_aa_bc<S, C, BC_INFLOW>(A, odd, nelem, blocks, st); break;
         default: return set_error(BGK_ERR_ARG, "AA lattices need a boundary case");
     }
     return check_launch(odd ? "aa_odd_kernel" : "aa_even_kernel");
@@ -186,21 +224,32 @@ int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n,
 
 }  // namespace bgk
 
-#define BGK_INSTANTIATE(S, C)                                                                      \
+// Explicit instantiations, split so that the kernel variants of one storage
+// kind compile in parallel translation units.
+#define BGK_INSTANTIATE_AB(S, C)                                                                   \
     namespace bgk {                                                                                \
     template int launch_sweep<S, C>(const bgk_sweep_params*, void* const*, void* const*, double*,  \
                                     cudaStream_t);                                                 \
-    template int launch_moments<S, C>(const bgk_sweep_params*, void* const*, double*, double*,     \
-                                      cudaStream_t);                                               \
-    template int launch_draglift<S, C>(const bgk_sweep_params*, void* const*, int, int, int, int,  \
-                                       int, int, double*, double*, size_t, cudaStream_t);          \
+    }
+#define BGK_INSTANTIATE_AA(S, C)                                                                   \
+    namespace bgk {                                                                                \
     template int launch_aa<S, C>(const bgk_sweep_params*, void* const*, bool, double*,             \
                                  cudaStream_t);                                                    \
-    template int launch_aa_prepass<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);     \
+    }
+#define BGK_INSTANTIATE_BATCH(S, C)                                                                \
+    namespace bgk {                                                                                \
     template size_t fill_batch_desc<S, C>(const bgk_sweep_params*, void* const*, void* const*,     \
                                           void*, uint32_t*);                                       \
     template int launch_batch<S, C>(const void*, const uint32_t*, int, uint32_t, unsigned*, int,   \
                                     int, int, cudaStream_t);                                       \
+    }
+#define BGK_INSTANTIATE_MISC(S, C)                                                                 \
+    namespace bgk {                                                                                \
+    template int launch_moments<S, C>(const bgk_sweep_params*, void* const*, double*, double*,     \
+                                      cudaStream_t);                                               \
+    template int launch_draglift<S, C>(const bgk_sweep_params*, void* const*, int, int, int, int,  \
+                                       int, int, double*, double*, size_t, cudaStream_t);          \
+    template int launch_aa_prepass<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);     \
     template int launch_outflow<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);        \
     template int launch_init<S, C>(void* const*, long long, long long, int, int, int, int,          \
                                    const double*, float, cudaStream_t);                            \

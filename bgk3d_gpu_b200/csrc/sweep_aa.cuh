@@ -31,27 +31,6 @@
 
 namespace bgk {
 
-// Outflow equilibria e = 9..13 (pops 10..14) from the stored populations
-// a[] of node (l, j, k) at rho = 1 (SRC/bcond.inflow.F90:135-162).
-template <class C>
-__device__ __forceinline__ void outflow_eq(const C (&a)[19], C cte1, const ColConst<C>& K, C (&eq)[5]) {
-    const C rhoinv = C(1), crho = C(1), rf = K.rf, qf = K.qf, three = C(3), p1 = K.p1, p2 = K.p2;
-    const C xj = (a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13]) * rhoinv;
-    const C yj = (a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17]) * rhoinv;
-    const C zj = (a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15]) * rhoinv;
-    const C cvsq = xj * xj + yj * yj + zj * zj;
-    const C cx10 = rf * (-xj - yj) + qf * (three * (xj + yj) * (xj + yj) - cvsq);
-    const C cx11 = rf * (-xj - zj) + qf * (three * (xj + zj) * (xj + zj) - cvsq);
-    const C cx12 = rf * (-xj + yj) + qf * (three * (xj - yj) * (xj - yj) - cvsq);
-    const C cx13 = rf * (-xj + zj) + qf * (three * (xj - zj) * (xj - zj) - cvsq);
-    const C cx14 = rf * (-xj) + qf * (three * (xj) * (xj) - cvsq);
-    eq[0] = crho * p2 * (cte1 + cx10);
-    eq[1] = crho * p2 * (cte1 + cx11);
-    eq[2] = crho * p2 * (cte1 + cx12);
-    eq[3] = crho * p2 * (cte1 + cx13);
-    eq[4] = crho * p1 * (cte1 + cx14);
-}
-
 // Node of this thread under the warp-segment mapping of sweep_ab_kernel;
 // returns false for idle lanes.
 template <class S, class C, class IDX>
@@ -72,57 +51,61 @@ __device__ __forceinline__ bool aa_node(const SweepArgs<S, C>& P, int& i, int& j
     return true;
 }
 
-// Even (local) step.  P.a and P.b both name the slot arrays.
-template <class S, class C, int BC, class IDX, bool GENERIC>
+// Even (local) step.  P.a and P.b both name the slot arrays.  Arithmetic in
+// storage units, as in sweep_node.
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
     int i, j, k;
     IDX c;
     if (!aa_node<S, C, IDX>(P, i, j, k, c)) return;
-    if (P.obs != nullptr && i >= P.imin && i <= P.imax && j >= P.jmin && j <= P.jmax && k >= P.kmin &&
-        k <= P.kmax && (obstacle_links(P, i, j, k) & 0x80000000u))
+    if (OBS && P.obs != nullptr && i >= P.imin && i <= P.imax && j >= P.jmin && j <= P.jmax &&
+        k >= P.kmin && k <= P.kmax && (obstacle_links(P, i, j, k) & 0x80000000u))
         return;
     S** f = const_cast<S**>(P.a);
-    const float inv = P.inv_scale, scl = P.scale;
+    const float inv = P.inv_scale;
     C x[19];
 #pragma unroll
-    for (int d = 0; d < 19; ++d) x[d] = Conv<S, C>::ld(f[d][c], inv);
+    for (int d = 0; d < 19; ++d) x[d] = Conv<S, C>::raw(f[d][c]);
     C y[19];
-    bgk_collide<C, GENERIC>(x, y, P.col);
+    collide_cm<S, C, CM>(x, y, P.col, P.fc, inv);
     S st[19];
 #pragma unroll
-    for (int d = 0; d < 19; ++d) st[d] = Conv<S, C>::st(y[d], scl);
+    for (int d = 0; d < 19; ++d) st[d] = Conv<S, C>::pack(y[d]);
 #pragma unroll
     for (int d = 0; d < 19; ++d) f[opp_of(d)][c] = st[d];
-    if ((BC == BC_INFLOW && i == P.l) || P.mom != nullptr) {
+    if (BC == BC_INFLOW && i == P.l) {
+        C s[19];
+#pragma unroll
+        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::raw(st[d]);
+        C eq[5];
+        outflow_eq<C, Scaled<S>::value>(s, P.inflow_cte1, P.col, inv, eq);
+#pragma unroll
+        for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::pack(eq[e]);
+    }
+    if (P.mom != nullptr) {
         C s[19];
 #pragma unroll
         for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(st[d], inv);
-        if (BC == BC_INFLOW && i == P.l) {
-            C eq[5];
-            outflow_eq<C>(s, P.inflow_cte1, P.col, eq);
-#pragma unroll
-            for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::st(eq[e], scl);
-        }
-        if (P.mom != nullptr) diagno_node<C>(s, P.col.cte1, m5);
+        diagno_node<C>(s, P.col.cte1, m5);
     }
 }
 
-template <class S, class C, int BC, class IDX, bool GENERIC>
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    aa_even_node<S, C, BC, IDX, GENERIC>(P, m5);
+    aa_even_node<S, C, BC, IDX, CM, OBS>(P, m5);
     if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 
 // Odd (pull + push) step.
-template <class S, class C, int BC, class IDX, bool GENERIC>
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
     typedef Faces<BC> F;
     int i, j, k;
     IDX c;
     if (!aa_node<S, C, IDX>(P, i, j, k, c)) return;
     uint32_t sl = 0;
-    if (P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
+    if (OBS && P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
         j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1) {
         sl = obstacle_links(P, i, j, k);
         if (sl & 0x80000000u) return;
@@ -140,7 +123,7 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
     const bool wxm = F::WX && i == 1, wxp = F::WX && i == P.l;
     const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
     const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
-    const float inv = P.inv_scale, scl = P.scale;
+    const float inv = P.inv_scale;
     C x[19];
 #pragma unroll
     for (int d = 0; d < 18; ++d) {
@@ -150,20 +133,23 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
         if (cx == 1) off += oxm; else if (cx == -1) off += oxp;
         if (cy == 1) off += oym; else if (cy == -1) off += oyp;
         if (cz == 1) off += ozm; else if (cz == -1) off += ozp;
-        bool bounce = ((sl >> d) & 1u) != 0;
+        bool bounce = OBS && ((sl >> d) & 1u) != 0;
         if (cx == 1) bounce |= wxm; else if (cx == -1) bounce |= wxp;
         if (cy == 1) bounce |= wym; else if (cy == -1) bounce |= wyp;
         if (cz == 1) bounce |= wzm; else if (cz == -1) bounce |= wzp;
-        C v = Conv<S, C>::ld(bounce ? f[d][c] : f[opp_of(d)][off], inv);
+        C v = Conv<S, C>::raw(bounce ? f[d][c] : f[opp_of(d)][off]);
         if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
-            v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force, scl, inv);
+            v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force);
         if (BC == BC_INFLOW && cx == 1 && i == 1)
-            v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col), scl, inv);
+            v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
         x[d] = v;
     }
-    x[18] = Conv<S, C>::ld(f[18][c], inv);
+    x[18] = Conv<S, C>::raw(f[18][c]);
     C y[19];
-    bgk_collide<C, GENERIC>(x, y, P.col);
+    collide_cm<S, C, CM>(x, y, P.col, P.fc, inv);
+    S sv[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) sv[d] = Conv<S, C>::pack(y[d]);
 #pragma unroll
     for (int d = 0; d < 18; ++d) {
         const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d), od = opp_of(d);
@@ -172,56 +158,55 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
         if (cx == 1) off += oxp; else if (cx == -1) off += oxm;
         if (cy == 1) off += oyp; else if (cy == -1) off += oym;
         if (cz == 1) off += ozp; else if (cz == -1) off += ozm;
-        bool bounce = ((sl >> od) & 1u) != 0;
+        bool bounce = OBS && ((sl >> od) & 1u) != 0;
         if (cx == 1) bounce |= wxp; else if (cx == -1) bounce |= wxm;
         if (cy == 1) bounce |= wyp; else if (cy == -1) bounce |= wym;
         if (cz == 1) bounce |= wzp; else if (cz == -1) bounce |= wzm;
-        const S sv = Conv<S, C>::st(y[d], scl);
         if (bounce) {
-            S bv = sv;
+            S bv = sv[d];
             if (BC == BC_DRIVEN && (od == 1 || od == 10) && k == P.n) {
-                const C r = Conv<S, C>::ld(sv, inv);
-                bv = Conv<S, C>::st(od == 1 ? r + P.lid_force : r - P.lid_force, scl);
+                const C r = Conv<S, C>::raw(sv[d]);
+                bv = Conv<S, C>::pack(od == 1 ? r + P.lid_force : r - P.lid_force);
             }
             f[od][c] = bv;
         } else {
             const bool gone = BC == BC_INFLOW && ((cx == -1 && i == 1) || (cx == 1 && i == P.l));
-            if (!gone) f[d][off] = sv;
+            if (!gone) f[d][off] = sv[d];
         }
     }
-    f[18][c] = Conv<S, C>::st(y[18], scl);
+    f[18][c] = sv[18];
     if (P.mom != nullptr) {
         C s[19];
 #pragma unroll
-        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(Conv<S, C>::st(y[d], scl), inv);
+        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(sv[d], inv);
         diagno_node<C>(s, P.col.cte1, m5);
     }
     if (BC == BC_INFLOW && i == 1) {
 #pragma unroll
         for (int d = 0; d < 5; ++d)
-            f[d][c] = Conv<S, C>::st(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col), scl);
+            f[d][c] = Conv<S, C>::pack(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
     }
     if (BC == BC_INFLOW && i == P.l) {
         C s[19];
 #pragma unroll
-        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(Conv<S, C>::st(y[d], scl), inv);
+        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::raw(sv[d]);
         C eq[5];
-        outflow_eq<C>(s, P.inflow_cte1, P.col, eq);
+        outflow_eq<C, Scaled<S>::value>(s, P.inflow_cte1, P.col, inv, eq);
 #pragma unroll
         for (int e = 0; e < 5; ++e) {
             const int d = 9 + e, cy = cy_of(d), cz = cz_of(d);
             IDX off = c;   // (l+1, j, k) + c_d = (l, j + c_y, k + c_z)
             if (cy == 1) off += oyp; else if (cy == -1) off += oym;
             if (cz == 1) off += ozp; else if (cz == -1) off += ozm;
-            f[d][off] = Conv<S, C>::st(eq[e], scl);
+            f[d][off] = Conv<S, C>::pack(eq[e]);
         }
     }
 }
 
-template <class S, class C, int BC, class IDX, bool GENERIC>
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    aa_odd_node<S, C, BC, IDX, GENERIC>(P, m5);
+    aa_odd_node<S, C, BC, IDX, CM, OBS>(P, m5);
     if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 
@@ -234,14 +219,13 @@ __global__ void aa_outflow_prepass_kernel(const SweepArgs<S, C> P) {
     if (j > P.m) return;
     S** f = const_cast<S**>(P.a);
     const long long c = (long long)P.l + P.nx * (long long)j + P.nxy * (long long)k;
-    const float inv = P.inv_scale, scl = P.scale;
     C s[19];
 #pragma unroll
-    for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(f[opp_of(d)][c], inv);
+    for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::raw(f[opp_of(d)][c]);
     C eq[5];
-    outflow_eq<C>(s, P.inflow_cte1, P.col, eq);
+    outflow_eq<C, Scaled<S>::value>(s, P.inflow_cte1, P.col, P.inv_scale, eq);
 #pragma unroll
-    for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::st(eq[e], scl);
+    for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::pack(eq[e]);
 }
 
 }  // namespace bgk

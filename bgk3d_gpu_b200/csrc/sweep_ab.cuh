@@ -21,7 +21,8 @@
 //   * a solid neighbour (obs==1) -> own opposite population.
 // Values that the reference constructs arithmetically before storing them in
 // the halo (lid, inflow) are rounded through the storage type, so 16-bit and
-// mixed kinds see exactly the reference's stored value.
+// mixed kinds see exactly the reference's stored value.  All arithmetic is in
+// storage units (Conv::raw / Conv::pack; the constants carry the scale).
 //
 // Solid nodes are not updated (their reference values are racy garbage: see
 // SRC/bcond_gpu.hpp:438-455).  An obstacle must keep one node away from the
@@ -38,8 +39,9 @@ template <class S, class C> struct SweepArgs {
     S* b[19];         // next populations; b[18] is ignored (pop 19 stays in a)
     long long nx, nxy;
     int l, m, n;
-    ColConst<C> col;
-    C lid_force;      // driven: added to pop 02 / subtracted from pop 11 at z = n+1
+    ColConst<C> col;  // storage units: p0, p1, p2, fx, fy, fz carry the scale
+    FastConst<C> fc;  // constants of the fused-multiply-add collision
+    C lid_force;      // driven, storage units: added to pop 02 / subtracted from pop 11 at z = n+1
     C u_inflow;       // inflow: prescribed x velocity at x = 0
     C inflow_cte1;    // inflow equilibrium constant (0 for shifted storage)
     float scale, inv_scale;
@@ -55,10 +57,12 @@ template <class S, class C> struct SweepArgs {
     double* mom;           // optional: per-block FP64 partial moments of the new state
     int bcase;             // BC_* (used by the batched kernel, which dispatches per tile)
     int generic;           // 1 unless the force-free shifted collision applies
+    int fast;              // 1: fused-multiply-add collision (float compute only)
 };
 
 // Equilibrium population p (0..4 -> 01..05) of the inflow face
-// (SRC/bcond.inflow.F90:165-181), in the compute type.
+// (SRC/bcond.inflow.F90:165-181), in the compute type (storage units when K
+// carries the scale).
 template <class C>
 __device__ __forceinline__ C inflow_eq(int p, C u_in, C cte1, const ColConst<C>& K) {
     const C rf = K.rf, qf = K.qf, three = C(3), crho = C(1);
@@ -76,9 +80,35 @@ __device__ __forceinline__ C inflow_eq(int p, C u_in, C cte1, const ColConst<C>&
     return crho * w * (cte1 + cxp);
 }
 
+// A value rounded to storage precision, as the reference's halo store rounds it.
 template <class S, class C>
-__device__ __forceinline__ C roundtrip(C v, float scl, float inv) {
-    return Conv<S, C>::ld(Conv<S, C>::st(v, scl), inv);
+__device__ __forceinline__ C roundtrip(C v) {
+    return Conv<S, C>::raw(Conv<S, C>::pack(v));
+}
+
+// Outflow equilibria e = 9..13 (pops 10..14) from the stored populations
+// a[] (storage units) of node (l, j, k) at rho = 1
+// (SRC/bcond.inflow.F90:135-162).
+template <class C, bool SCALED>
+__device__ __forceinline__ void outflow_eq(const C (&a)[19], C cte1, const ColConst<C>& K, float inv,
+                                           C (&eq)[5]) {
+    const C rhoinv = C(1), crho = C(1), rf = K.rf, qf = K.qf, three = C(3), p1 = K.p1, p2 = K.p2;
+    C mx = a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13];
+    C my = a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17];
+    C mz = a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15];
+    if (SCALED) { mx = mx * (C)inv; my = my * (C)inv; mz = mz * (C)inv; }
+    const C xj = mx * rhoinv, yj = my * rhoinv, zj = mz * rhoinv;
+    const C cvsq = xj * xj + yj * yj + zj * zj;
+    const C cx10 = rf * (-xj - yj) + qf * (three * (xj + yj) * (xj + yj) - cvsq);
+    const C cx11 = rf * (-xj - zj) + qf * (three * (xj + zj) * (xj + zj) - cvsq);
+    const C cx12 = rf * (-xj + yj) + qf * (three * (xj - yj) * (xj - yj) - cvsq);
+    const C cx13 = rf * (-xj + zj) + qf * (three * (xj - zj) * (xj - zj) - cvsq);
+    const C cx14 = rf * (-xj) + qf * (three * (xj) * (xj) - cvsq);
+    eq[0] = crho * p2 * (cte1 + cx10);
+    eq[1] = crho * p2 * (cte1 + cx11);
+    eq[2] = crho * p2 * (cte1 + cx12);
+    eq[3] = crho * p2 * (cte1 + cx13);
+    eq[4] = crho * p1 * (cte1 + cx14);
 }
 
 // Compile-time description of the six faces of a boundary case.
@@ -118,7 +148,9 @@ __device__ __forceinline__ uint32_t obstacle_links(const SweepArgs<S, C>& P, int
 // make every store and every c_x = 0 load a whole number of 32-byte sectors.
 // One thread per node; blocks of 256 threads = 8 row segments.
 // gw: this warp's global segment index within the lattice.
-template <class S, class C, int BC, class IDX, bool GENERIC>
+// CM: collision mode; OBS: the lattice may have an obstacle (P.obs is then
+// tested at run time; OBS = false compiles the obstacle logic out).
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
     typedef Faces<BC> F;
     const int lane = threadIdx.x & 31;
@@ -136,7 +168,7 @@ __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw
     const IDX c = rowoff + (IDX)i;
 
     uint32_t sl = 0;
-    if (P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
+    if (OBS && P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
         j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1) {
         sl = obstacle_links(P, i, j, k);
         if (sl & 0x80000000u) return;   // solid node: not updated
@@ -162,25 +194,24 @@ __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw
         if (cx == 1) off += oxm; else if (cx == -1) off += oxp;
         if (cy == 1) off += oym; else if (cy == -1) off += oyp;
         if (cz == 1) off += ozm; else if (cz == -1) off += ozp;
-        bool bounce = ((sl >> d) & 1u) != 0;
+        bool bounce = OBS && ((sl >> d) & 1u) != 0;
         if (cx == 1) bounce |= wxm; else if (cx == -1) bounce |= wxp;
         if (cy == 1) bounce |= wym; else if (cy == -1) bounce |= wyp;
         if (cz == 1) bounce |= wzm; else if (cz == -1) bounce |= wzp;
         const S* src = bounce ? P.a[opp_of(d)] : P.a[d];
-        C v = Conv<S, C>::ld(ldro<S>(src + (bounce ? c : off)), inv);
+        C v = Conv<S, C>::raw(ldro<S>(src + (bounce ? c : off)));
         if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
-            v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force, P.scale, inv);
+            v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force);
         if (BC == BC_INFLOW && cx == 1 && i == 1)
-            v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col), P.scale, inv);
+            v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
         x[d] = v;
     }
-    x[18] = Conv<S, C>::ld(P.a[18][c], inv);
+    x[18] = Conv<S, C>::raw(P.a[18][c]);
     C y[19];
-    bgk_collide<C, GENERIC>(x, y, P.col);
-    const float scl = P.scale;
+    collide_cm<S, C, CM>(x, y, P.col, P.fc, inv);
     S sv[19];
 #pragma unroll
-    for (int d = 0; d < 19; ++d) sv[d] = Conv<S, C>::st(y[d], scl);
+    for (int d = 0; d < 19; ++d) sv[d] = Conv<S, C>::pack(y[d]);
 #pragma unroll
     for (int d = 0; d < 18; ++d) P.b[d][c] = sv[d];
     const_cast<S*>(P.a[18])[c] = sv[18];
@@ -195,10 +226,10 @@ __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw
 // One launch = one time step.  With P.mom set, every block also writes the
 // FP64 sums of SRC/diagno.F90's per-node moments of the state it produced
 // (fluid nodes) to P.mom[blockIdx.x * 5 ..].
-template <class S, class C, int BC, class IDX, bool GENERIC>
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) sweep_ab_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    sweep_node<S, C, BC, IDX, GENERIC>(P, blockIdx.x * 8u + (threadIdx.x >> 5), m5);
+    sweep_node<S, C, BC, IDX, CM, OBS>(P, blockIdx.x * 8u + (threadIdx.x >> 5), m5);
     if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 
@@ -211,29 +242,16 @@ __global__ void outflow_halo_kernel(const SweepArgs<S, C> P) {
     const int j = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int k = 1 + (int)blockIdx.y;
     if (j > P.m) return;
-    const float inv = P.inv_scale, scl = P.scale;
     const long long c = (long long)P.l + P.nx * (long long)j + P.nxy * (long long)k;
     C a[19];
 #pragma unroll
-    for (int d = 0; d < 19; ++d) a[d] = Conv<S, C>::ld(P.a[d][c], inv);
-    const C rhoinv = C(1), crho = C(1), rf = P.col.rf, qf = P.col.qf, three = C(3);
-    const C cte1 = P.inflow_cte1, p1 = P.col.p1, p2 = P.col.p2;
-    const C xj = (a[0] + a[1] + a[2] + a[3] + a[4] - a[9] - a[10] - a[11] - a[12] - a[13]) * rhoinv;
-    const C yj = (a[2] + a[6] + a[7] + a[8] + a[11] - a[0] - a[9] - a[15] - a[16] - a[17]) * rhoinv;
-    const C zj = (a[3] + a[5] + a[6] + a[12] + a[17] - a[1] - a[8] - a[10] - a[14] - a[15]) * rhoinv;
-    const C cvsq = xj * xj + yj * yj + zj * zj;
-    const C cx10 = rf * (-xj - yj) + qf * (three * (xj + yj) * (xj + yj) - cvsq);
-    const C cx11 = rf * (-xj - zj) + qf * (three * (xj + zj) * (xj + zj) - cvsq);
-    const C cx12 = rf * (-xj + yj) + qf * (three * (xj - yj) * (xj - yj) - cvsq);
-    const C cx13 = rf * (-xj + zj) + qf * (three * (xj - zj) * (xj - zj) - cvsq);
-    const C cx14 = rf * (-xj) + qf * (three * (xj) * (xj) - cvsq);
+    for (int d = 0; d < 19; ++d) a[d] = Conv<S, C>::raw(P.a[d][c]);
+    C eq[5];
+    outflow_eq<C, Scaled<S>::value>(a, P.inflow_cte1, P.col, P.inv_scale, eq);
     const long long h = c + 1;
     S** A = const_cast<S**>(P.a);
-    A[9][h] = Conv<S, C>::st(crho * p2 * (cte1 + cx10), scl);
-    A[10][h] = Conv<S, C>::st(crho * p2 * (cte1 + cx11), scl);
-    A[11][h] = Conv<S, C>::st(crho * p2 * (cte1 + cx12), scl);
-    A[12][h] = Conv<S, C>::st(crho * p2 * (cte1 + cx13), scl);
-    A[13][h] = Conv<S, C>::st(crho * p1 * (cte1 + cx14), scl);
+#pragma unroll
+    for (int e = 0; e < 5; ++e) A[9 + e][h] = Conv<S, C>::pack(eq[e]);
 }
 
 }  // namespace bgk

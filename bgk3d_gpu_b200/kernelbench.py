@@ -1,0 +1,102 @@
+"""Time-step throughput of library-owned lattices per storage kind, access
+pattern and boundary case (CUDA events on the launching stream; inputs larger
+than L2 for the default size, so no flush is needed).
+
+  python -m bgk3d_gpu_b200.kernelbench [--kinds f32,f16] [--patterns ab,aa]
+        [--cases periodic,driven] [--size 256 256 256] [--steps 200] [--warmup 20]
+
+One JSON line per combination: GLUPS, ms per step, algorithmic HBM GB/s
+(2 x 19 x bytes per value per update) and its fraction of the measured copy
+bandwidth.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+import torch
+
+from . import cases as CS
+from .lattice import Lattice
+
+BYTES = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2, "f32f64": 4}
+
+
+def peak_gbs() -> float | None:
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def make(kind: str, pattern: str, case: str, l: int, m: int, n: int, fast: bool = False) -> Lattice:
+    kw = dict(kind=kind, pattern=pattern, scale=256.0 if kind == "f16" else 1.0, fast=fast)
+    omega = 1.0 / 0.524
+    if case == "periodic":
+        lat = Lattice(l, m, n, bcase="periodic", omega=omega, **kw)
+        lat.init_flow("tgv", (0.05,))
+    elif case == "driven":
+        lat = Lattice(l, m, n, bcase="driven", omega=omega, lid_force=0.1 / 6.0, **kw)
+        lat.init_flow("rest")
+    elif case == "channel":
+        lat = Lattice(l, m, n, bcase="channel", omega=omega, force_mode=1, force=(1e-7, 0.0, 0.0), **kw)
+        lat.init_flow("rest")
+    elif case == "inflow":
+        lat = Lattice(l, m, n, bcase="inflow", omega=omega, u_inflow=0.05, **kw)
+        obs, _ = CS.solid_sphere_obstacle(l, m, n, min(40.0, m / 4), (l // 4, m // 2, n // 2))
+        lat.set_obstacle(obs)
+        lat.init_flow("rest")
+    else:
+        raise ValueError(case)
+    return lat
+
+
+def time_steps(lat: Lattice, steps: int, warmup: int) -> float:
+    """Seconds per step over `steps` steps after `warmup` steps."""
+    lat.step(warmup)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    lat.step(steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / steps
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--kinds", default="f32,f16,bf16,f64")
+    ap.add_argument("--patterns", default="ab")
+    ap.add_argument("--cases", default="periodic")
+    ap.add_argument("--size", type=int, nargs=3, default=[256, 256, 256])
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--modes", default="strict", help="collision modes: strict, fast or both (strict,fast)")
+    args = ap.parse_args(argv)
+    l, m, n = args.size
+    peak = peak_gbs()
+    for case in args.cases.split(","):
+        for pattern in args.patterns.split(","):
+            for kind in args.kinds.split(","):
+                for mode in args.modes.split(","):
+                    if mode == "fast" and kind in ("f64", "f32f64"):
+                        continue        # fused collision: float compute only
+                    lat = make(kind, pattern, case, l, m, n, fast=(mode == "fast"))
+                    s = time_steps(lat, args.steps, args.warmup)
+                    lat.close()
+                    glups = l * m * n / s / 1e9
+                    gbs = glups * 2 * 19 * BYTES[kind]
+                    print(json.dumps({"kind": kind, "mode": mode, "pattern": pattern, "case": case,
+                                      "size": [l, m, n], "steps": args.steps, "ms_per_step": s * 1e3,
+                                      "glups": glups, "hbm_gbs": gbs,
+                                      "frac_of_measured": gbs / peak if peak else None}), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

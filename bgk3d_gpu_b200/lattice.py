@@ -34,7 +34,7 @@ class DeviceLattice:
 
     def __init__(self, l, m, n, kind="f32", bcase="periodic", omega=1.0, ipad=0, jpad=0,
                  device="cuda", scale=1.0, lid_force=0.0, u_inflow=0.0, inflow_cte1=0.0,
-                 force_mode=0, force=(0.0, 0.0, 0.0), cte1=1.0):
+                 force_mode=0, force=(0.0, 0.0, 0.0), cte1=1.0, fast=False):
         self.l, self.m, self.n = l, m, n
         self.kind, self.bcase = _kind(kind), _bcase(bcase)
         self.nx, self.ny, self.nz = l + 2 + ipad, m + 2 + jpad, n + 2
@@ -49,7 +49,7 @@ class DeviceLattice:
                                    ny=self.ny, scale=scale, lid_force=lid_force, u_inflow=u_inflow,
                                    inflow_cte1=inflow_cte1, force_mode=force_mode,
                                    fx=force[0], fy=force[1], fz=force[2], cte1=cte1,
-                                   cte0=1.0 - cte1)
+                                   cte0=1.0 - cte1, fast=1 if fast else 0)
         self._ws = None
         self._out = torch.zeros(8, dtype=torch.float64, device=self.device)
         self.steps_done = 0
@@ -162,7 +162,7 @@ class Lattice:
 
     def __init__(self, l, m, n, kind="f32", bcase="periodic", omega=1.0, pattern="ab",
                  lid_force=0.0, u_inflow=0.0, force_mode=0, force=(0.0, 0.0, 0.0), scale=1.0,
-                 device=None):
+                 device=None, fast=False):
         from ._lattice_abi import LatticeDesc
         self.L = lib()
         self.l, self.m, self.n = l, m, n
@@ -174,6 +174,7 @@ class Lattice:
         d.lid_force, d.u_inflow, d.force_mode = lid_force, u_inflow, force_mode
         d.fx, d.fy, d.fz = force
         d.scale = scale
+        d.fast = 1 if fast else 0
         self.desc = d
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):

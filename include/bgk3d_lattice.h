@@ -38,9 +38,10 @@ typedef struct bgk_lattice_desc {
     double lid_force;      /* DRIVEN: u_lid / 6 */
     double u_inflow;       /* INFLOW */
     float scale;           /* 16-bit kinds: power-of-two storage scale */
+    int fast;              /* bgk_sweep_params.fast: 1 = fused-multiply-add collision */
 } bgk_lattice_desc;
 
-/* Defaults: AB pattern, no force, lid 0, inflow 0, scale 1. */
+/* Defaults: AB pattern, no force, lid 0, inflow 0, scale 1, fast 0. */
 void bgk_lattice_desc_init(bgk_lattice_desc* d, int kind, int bcase, int l, int m, int n, double omega);
 
 /* Device bytes a lattice with this description occupies (admission control). */
