@@ -66,6 +66,12 @@ def bind(L) -> None:
     L.bgk_lattice_probe.restype = c_int
     L.bgk_lattice_slice.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p]
     L.bgk_lattice_slice.restype = c_int
+    L.bgk_lattice_uses_tma.argtypes = [c_void_p]
+    L.bgk_lattice_uses_tma.restype = c_int
+    L.bgk_set_tma_kernels.argtypes = [c_int]
+    L.bgk_set_tma_kernels.restype = c_int
+    L.bgk_lattice_status.argtypes = [c_void_p]
+    L.bgk_lattice_status.restype = c_int
     L.bgk_lattice_init.argtypes = [c_void_p, c_int, c_void_p, c_void_p]
     L.bgk_lattice_init.restype = c_int
     L.bgk_lattice_load.argtypes = [c_void_p, c_void_p, c_void_p]

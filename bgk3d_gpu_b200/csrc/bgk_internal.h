@@ -5,6 +5,10 @@
 #include "bgk3d_b200.h"
 
 namespace bgk {
+// TMA-staged sweep switch for library-owned lattices (bgk_set_tma_kernels).
+// Off by default: bit-exact, 280 instead of 408 instructions per node for
+// FP16, but measured at half the one-node kernel's rate on 256^3 (B200).
+inline bool g_tma_kernels = false;
 // Record a formatted message as the calling thread's last error; returns code.
 int set_error(int code, const char* fmt, ...);
 // cudaGetLastError after a launch, recorded as an error when it failed.

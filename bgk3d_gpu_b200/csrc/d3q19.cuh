@@ -143,48 +143,47 @@ __host__ __device__ constexpr bool cm_fast(int cm) { return cm >= 2; }
 // cte0 = 0) without forcing: it omits the terms that are then additions of
 // +0 or multiplications by 1, which changes no result except possibly the
 // sign of an exact zero.
-template <class C, bool GENERIC = true, bool SCALED = false>
-__device__ __forceinline__ void bgk_collide(const C (&x)[19], C (&y)[19], const ColConst<C>& P,
-                                            float inv = 1.0f) {
-    const C cte0 = P.cte0, cte1 = P.cte1, tre = P.tre, qf = P.qf, rf = P.rf;
-    C sum = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] +
+template <class V, class C, bool GENERIC, bool SCALED>
+__device__ __forceinline__ void bgk_collide_v(const V (&x)[19], V (&y)[19], const ColConst<C>& P, float inv) {
+    const V cte0 = V(P.cte0), cte1 = V(P.cte1), tre = V(P.tre), qf = V(P.qf), rf = V(P.rf);
+    V sum = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] +
             x[11] + x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18];
-    if (SCALED) sum = sum * (C)inv;
-    const C rho = sum + cte1;
-    const C rhoinv = C(1) / rho;
-    C mx = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
-    C my = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
-    C mz = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
-    if (SCALED) { mx = mx * (C)inv; my = my * (C)inv; mz = mz * (C)inv; }
-    C vx = mx * rhoinv, vy = my * rhoinv, vz = mz * rhoinv;
-    const C vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
-    const C vsq = vx2 + vy2 + vz2;
-    auto q = [&](C t) -> C { return GENERIC ? cte0 + qf * t : qf * t; };
-    C vxpy = vx + vy;
-    const C qxpy = q(tre * vxpy * vxpy - vsq);
-    C vxmy = vx - vy;
-    const C qxmy = q(tre * vxmy * vxmy - vsq);
-    C vxpz = vx + vz;
-    const C qxpz = q(tre * vxpz * vxpz - vsq);
-    C vxmz = vx - vz;
-    const C qxmz = q(tre * vxmz * vxmz - vsq);
-    C vypz = vy + vz;
-    const C qypz = q(tre * vypz * vypz - vsq);
-    C vymz = vy - vz;
-    const C qymz = q(tre * vymz * vymz - vsq);
-    const C qx = q(tre * vx2 - vsq);
-    const C qy = q(tre * vy2 - vsq);
-    const C qz = q(tre * vz2 - vsq);
-    const C q0 = q(-vsq);
+    if (SCALED) sum = sum * V((C)inv);
+    const V rho = sum + cte1;
+    const V rhoinv = V(C(1)) / rho;
+    V mx = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
+    V my = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
+    V mz = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
+    if (SCALED) { mx = mx * V((C)inv); my = my * V((C)inv); mz = mz * V((C)inv); }
+    V vx = mx * rhoinv, vy = my * rhoinv, vz = mz * rhoinv;
+    const V vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
+    const V vsq = vx2 + vy2 + vz2;
+    auto q = [&](V t) -> V { return GENERIC ? cte0 + qf * t : qf * t; };
+    V vxpy = vx + vy;
+    const V qxpy = q(tre * vxpy * vxpy - vsq);
+    V vxmy = vx - vy;
+    const V qxmy = q(tre * vxmy * vxmy - vsq);
+    V vxpz = vx + vz;
+    const V qxpz = q(tre * vxpz * vxpz - vsq);
+    V vxmz = vx - vz;
+    const V qxmz = q(tre * vxmz * vxmz - vsq);
+    V vypz = vy + vz;
+    const V qypz = q(tre * vypz * vypz - vsq);
+    V vymz = vy - vz;
+    const V qymz = q(tre * vymz * vymz - vsq);
+    const V qx = q(tre * vx2 - vsq);
+    const V qy = q(tre * vy2 - vsq);
+    const V qz = q(tre * vz2 - vsq);
+    const V q0 = q(-vsq);
     vx = rf * vx; vy = rf * vy; vz = rf * vz;
     vxpy = rf * vxpy; vxmy = rf * vxmy; vxpz = rf * vxpz;
     vxmz = rf * vxmz; vypz = rf * vypz; vymz = rf * vymz;
-    const C p0 = P.p0, p1 = P.p1, p2 = P.p2;
-    const C rp0 = rho * p0, rp1 = rho * p1, rp2 = rho * p2;
-    const C s2 = GENERIC ? cte1 * (rp2 - p2) : rp2 - p2;
-    const C s1 = GENERIC ? cte1 * (rp1 - p1) : rp1 - p1;
-    const C s0 = GENERIC ? cte1 * (rp0 - p0) : rp0 - p0;
-    C e[19];
+    const V p0 = V(P.p0), p1 = V(P.p1), p2 = V(P.p2);
+    const V rp0 = rho * p0, rp1 = rho * p1, rp2 = rho * p2;
+    const V s2 = GENERIC ? cte1 * (rp2 - p2) : rp2 - p2;
+    const V s1 = GENERIC ? cte1 * (rp1 - p1) : rp1 - p1;
+    const V s0 = GENERIC ? cte1 * (rp0 - p0) : rp0 - p0;
+    V e[19];
     e[0] = rp2 * (+vxmy + qxmy) + s2;
     e[1] = rp2 * (+vxmz + qxmz) + s2;
     e[2] = rp2 * (+vxpy + qxpy) + s2;
@@ -204,13 +203,13 @@ __device__ __forceinline__ void bgk_collide(const C (&x)[19], C (&y)[19], const 
     e[16] = rp1 * (-vy + qy) + s1;
     e[17] = rp2 * (-vymz + qymz) + s2;
     e[18] = rp0 * (+q0) + s0;
-    const C om = P.omega;
+    const V om = V(P.omega);
     if (!GENERIC) {
 #pragma unroll
         for (int d = 0; d < 18; ++d) y[d] = x[d] - om * (x[d] - e[d]);
     } else {
-    C fx = P.fx, fy = P.fy, fz = P.fz;
-    if (P.force_mode == 1) { fx = P.fx * rho; fy = P.fy * rho; fz = P.fz * rho; }
+    V fx = V(P.fx), fy = V(P.fy), fz = V(P.fz);
+    if (P.force_mode == 1) { fx = V(P.fx) * rho; fy = V(P.fy) * rho; fz = V(P.fz) * rho; }
     y[0] = x[0] - om * (x[0] - e[0]) + fx - fy;
     y[1] = x[1] - om * (x[1] - e[1]) + fx - fz;
     y[2] = x[2] - om * (x[2] - e[2]) + fx + fy;
@@ -231,6 +230,13 @@ __device__ __forceinline__ void bgk_collide(const C (&x)[19], C (&y)[19], const 
     y[17] = x[17] - om * (x[17] - e[17]) - fy + fz;
     }
     y[18] = x[18] - om * (x[18] - e[18]);
+}
+
+// The collision on one node's compute values.
+template <class C, bool GENERIC = true, bool SCALED = false>
+__device__ __forceinline__ void bgk_collide(const C (&x)[19], C (&y)[19], const ColConst<C>& P,
+                                            float inv = 1.0f) {
+    bgk_collide_v<C, C, GENERIC, SCALED>(x, y, P, inv);
 }
 
 // Constants of the fused-multiply-add collision, in storage units, computed
@@ -262,32 +268,32 @@ __device__ __forceinline__ double rcp_c(double a) { return 1.0 / a; }
 // which is odd in c).  About 140 operations per node instead of 240; not
 // bit-identical to the reference order (the results differ by a few units in
 // the last place of the compute type per step).
-template <class C, bool GENERIC, bool SCALED>
-__device__ __forceinline__ void bgk_collide_fast(const C (&x)[19], C (&y)[19], const FastConst<C>& K,
-                                                 float inv = 1.0f) {
-    const C sum = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] + x[11] +
+template <class V, class C, bool GENERIC, bool SCALED>
+__device__ __forceinline__ void bgk_collide_fast_v(const V (&x)[19], V (&y)[19], const FastConst<C>& K,
+                                                   float inv) {
+    const V sum = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] + x[11] +
                   x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18];
-    const C rho = SCALED ? fma_c(sum, (C)inv, K.cte1) : sum + K.cte1;
-    const C ri = rcp_c(rho);
-    const C mx = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
-    const C my = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
-    const C mz = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
-    const C g = SCALED ? (C)inv * ri : ri;
-    const C vx = mx * g, vy = my * g, vz = mz * g;
-    const C vsq = fma_c(vz, vz, fma_c(vy, vy, vx * vx));
-    const C t = GENERIC ? fma_c(-K.qf, vsq, K.cte0) : -K.qf * vsq;
-    const C u = GENERIC ? fma_c(rho, t, K.cte1 * (rho - C(1))) : fma_c(rho, t, rho - C(1));
-    const C B0 = K.b0 * u, B1 = K.b1 * u, B2 = K.b2 * u;
-    const C A1 = rho * K.a1, A2 = rho * K.a2, R1 = rho * K.r1, R2 = rho * K.r2;
-    C fx = C(0), fy = C(0), fz = C(0);
+    const V rho = SCALED ? fma_c(sum, V((C)inv), V(K.cte1)) : sum + V(K.cte1);
+    const V ri = rcp_c(rho);
+    const V mx = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
+    const V my = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
+    const V mz = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
+    const V g = SCALED ? V((C)inv) * ri : ri;
+    const V vx = mx * g, vy = my * g, vz = mz * g;
+    const V vsq = fma_c(vz, vz, fma_c(vy, vy, vx * vx));
+    const V t = GENERIC ? fma_c(V(-K.qf), vsq, V(K.cte0)) : V(-K.qf) * vsq;
+    const V u = GENERIC ? fma_c(rho, t, V(K.cte1) * (rho - V(C(1)))) : fma_c(rho, t, rho - V(C(1)));
+    const V B0 = V(K.b0) * u, B1 = V(K.b1) * u, B2 = V(K.b2) * u;
+    const V A1 = rho * V(K.a1), A2 = rho * V(K.a2), R1 = rho * V(K.r1), R2 = rho * V(K.r2);
+    V fx = V(C(0)), fy = V(C(0)), fz = V(C(0));
     if (GENERIC) {
-        fx = K.fx; fy = K.fy; fz = K.fz;
+        fx = V(K.fx); fy = V(K.fy); fz = V(K.fz);
         if (K.force_mode == 1) { fx = fx * rho; fy = fy * rho; fz = fz * rho; }
     }
-    const C om = K.omc;
-    auto pair = [&](int dp, int dm, C v, C A, C B, C R, C f) {
-        const C sym = fma_c(A, v * v, B);
-        const C an = GENERIC ? fma_c(R, v, f) : R * v;
+    const V om = V(K.omc);
+    auto pair = [&](int dp, int dm, V v, V A, V B, V R, V f) {
+        const V sym = fma_c(A, v * v, B);
+        const V an = GENERIC ? fma_c(R, v, f) : R * v;
         y[dp] = fma_c(x[dp], om, sym) + an;
         y[dm] = fma_c(x[dm], om, sym) - an;
     };
@@ -301,6 +307,12 @@ __device__ __forceinline__ void bgk_collide_fast(const C (&x)[19], C (&y)[19], c
     pair(7, 16, vy, A1, B1, R1, fy);
     pair(8, 17, vy - vz, A2, B2, R2, fy - fz);
     y[18] = fma_c(x[18], om, B0);
+}
+
+template <class C, bool GENERIC, bool SCALED>
+__device__ __forceinline__ void bgk_collide_fast(const C (&x)[19], C (&y)[19], const FastConst<C>& K,
+                                                 float inv = 1.0f) {
+    bgk_collide_fast_v<C, C, GENERIC, SCALED>(x, y, K, inv);
 }
 
 // Collision of one node in storage units under collision mode CM.

@@ -1,0 +1,64 @@
+// Two FP32 values advanced together by the packed arithmetic of sm_100
+// (FADD2 / FFMA2: one instruction for both lanes, each lane rounded exactly
+// like the scalar operation), so that a collision written once for a value
+// type V runs on two nodes at the cost of one.
+//
+// A packed multiply followed by a packed add can be contracted into one fused
+// multiply-add by the code generator even when both carry an explicit
+// rounding mode (observed on B200 with CUDA 12.9: about a fifth of a*a + b*b
+// results one unit off), which would break the bit-exact parity with the
+// reference's operation order.  So a product is formed as fma(a, b, z) with
+// z = -0 read from constant memory: the compiler cannot know the addend,
+// a*b + (-0) rounds exactly like a*b, and the result is an ordinary rounded
+// value that a following addition cannot absorb.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+namespace bgk {
+
+static __constant__ float2 k_negzero2 = {-0.0f, -0.0f};
+
+struct F2 {
+    float2 v;
+    __device__ __forceinline__ F2() {}
+    __device__ __forceinline__ explicit F2(float s) : v(make_float2(s, s)) {}
+    __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
+    __device__ __forceinline__ explicit F2(float2 w) : v(w) {}
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(__fadd2_rn(a.v, b.v)); }
+__device__ __forceinline__ F2 operator-(F2 a) { return F2(make_float2(-a.v.x, -a.v.y)); }
+__device__ __forceinline__ F2 operator+(F2 a) { return a; }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y))); }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(__ffma2_rn(a.v, b.v, k_negzero2)); }
+__device__ __forceinline__ F2 operator/(F2 a, F2 b) {
+    return F2(__fdiv_rn(a.v.x, b.v.x), __fdiv_rn(a.v.y, b.v.y));
+}
+__device__ __forceinline__ F2 fma_c(F2 a, F2 b, F2 c) { return F2(__ffma2_rn(a.v, b.v, c.v)); }
+__device__ __forceinline__ F2 rcp_c(F2 a) { return F2(__frcp_rn(a.v.x), __frcp_rn(a.v.y)); }
+
+// Storage <-> two compute values (storage units), and the 2-element vectors.
+template <class S> struct Pack2;
+template <> struct Pack2<float> {
+    typedef float2 V;
+    static __device__ __forceinline__ F2 raw(V w) { return F2(w); }
+    static __device__ __forceinline__ V pack(F2 a) { return a.v; }
+    static __device__ __forceinline__ float lo(V w) { return w.x; }
+    static __device__ __forceinline__ float hi(V w) { return w.y; }
+};
+template <> struct Pack2<__half> {
+    typedef __half2 V;
+    static __device__ __forceinline__ F2 raw(V w) { return F2(__half22float2(w)); }
+    static __device__ __forceinline__ V pack(F2 a) { return __floats2half2_rn(a.v.x, a.v.y); }
+    static __device__ __forceinline__ __half lo(V w) { return __low2half(w); }
+    static __device__ __forceinline__ __half hi(V w) { return __high2half(w); }
+};
+template <> struct Pack2<__nv_bfloat16> {
+    typedef __nv_bfloat162 V;
+    static __device__ __forceinline__ F2 raw(V w) { return F2(__bfloat1622float2(w)); }
+    static __device__ __forceinline__ V pack(F2 a) { return __floats2bfloat162_rn(a.v.x, a.v.y); }
+    static __device__ __forceinline__ __nv_bfloat16 lo(V w) { return __low2bfloat16(w); }
+    static __device__ __forceinline__ __nv_bfloat16 hi(V w) { return __high2bfloat16(w); }
+};
+
+}  // namespace bgk

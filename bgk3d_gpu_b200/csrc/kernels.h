@@ -11,6 +11,9 @@ namespace bgk {
 template <class S, class C>
 int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st);
 template <class S, class C>
+int launch_sweep_tma(const bgk_sweep_params* p, void* const* a, void* const* b, const void* tmap, const int* pa,
+                     int* err, cudaStream_t st);
+template <class S, class C>
 int launch_moments(const bgk_sweep_params* p, void* const* a, double* out, double* ws, cudaStream_t st);
 template <class S, class C>
 int launch_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks, int ke,

@@ -1,6 +1,8 @@
 // Library-owned lattices (include/bgk3d_lattice.h): padded aligned layout,
 // AB and in-place AA time steps, CUDA-graph replay of long step runs,
 // host transfers in the reference layout, FP64 diagnostics.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstring>
@@ -12,6 +14,7 @@
 #include "kernels.h"
 #include "d3q19.cuh"
 #include "lattice_internal.h"
+#include "sweep_tma.cuh"
 
 using namespace bgk;
 
@@ -33,7 +36,11 @@ struct Geometry { long long nx, ny, nz, origin, plane; };
 
 Geometry geometry(const bgk_lattice_desc* d) {
     Geometry g;
-    g.nx = ((long long)d->l + 2 + 31) / 32 * 32;   // row pitch: whole 32-element segments
+    // row pitch: whole 32-element segments, and room for nodes 0..l at
+    // elements 31..l+31 of their own row (the TMA sweep's tensor map sees a
+    // row as nx elements; the halo node l+1 may spill into the next row's
+    // unused first element)
+    g.nx = ((long long)d->l + 32 + 31) / 32 * 32;
     g.ny = (long long)d->m + 2;
     g.nz = (long long)d->n + 2;
     g.origin = 31;                                   // node (1, j, k) on a segment boundary
@@ -62,12 +69,19 @@ int aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
 // AA: population p of the observable state lives in slot opp(p).
 // One time step on stream st (no graph); with mom, the FP64 partial moments
 // of the new state go to mom (one slot of 5 doubles per block).
+int tma_step(bgk_lattice* L, cudaStream_t st);
+
 int one_step(bgk_lattice* L, cudaStream_t st, double* mom = nullptr) {
     if (L->desc.pattern == BGK_PATTERN_AA) {
         const bool odd = (L->steps % 2) == 0;   // Layout E -> odd kernel
         if (int e = aa_step(&L->p, L->a, odd, mom, st)) return e;
     } else {
-        if (int e = sweep_launch_mom(&L->p, L->a, L->b, mom, st)) return e;
+        const bool has_obs = L->p.obs && L->p.imin <= L->p.imax;
+        if (!mom && L->tma_ok && g_tma_kernels && !has_obs) {
+            if (int e = tma_step(L, st)) return e;
+        } else if (int e = sweep_launch_mom(&L->p, L->a, L->b, mom, st)) {
+            return e;
+        }
         for (int d = 0; d < 18; ++d) std::swap(L->a[d], L->b[d]);
     }
     ++L->steps;
@@ -111,6 +125,65 @@ int ensure_workspace(const bgk_lattice* Lc) {
     if (e != cudaSuccess) return set_error(BGK_ERR_NOMEM, "workspace: %s", cudaGetErrorString(e));
     L->ws_bytes = need;
     return BGK_OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda); null when the driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+// The 4-D tensor map of an AB lattice's allocation for the TMA sweep: x over
+// the row pitch, y over m + 2 rows, z over n + 2 planes, w over the 37
+// population planes; box = (64 nodes + 16 bytes each side) x kTmaRows rows.
+void make_tensor_map(bgk_lattice* L) {
+    L->tma_ok = false;
+    if (L->desc.pattern != BGK_PATTERN_AB) return;
+    // float compute only (FP64 compute already reaches the HBM roofline)
+    if (L->desc.kind != K_F32 && L->desc.kind != K_F16 && L->desc.kind != K_BF16) return;
+    if (L->nx * L->ny * L->nz + 64 >= (1LL << 31)) return;   // the TMA kernel uses 32-bit offsets
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return;
+    CUtensorMapDataType dt;
+    int box_x;
+    switch (L->desc.kind) {
+        case K_F64: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT64; box_x = TmaBox<double>::W; break;
+        case K_F16: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; box_x = TmaBox<__half>::W; break;
+        case K_BF16: dt = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; box_x = TmaBox<__nv_bfloat16>::W; break;
+        default: dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; box_x = TmaBox<float>::W; break;
+    }
+    const cuuint64_t es = (cuuint64_t)L->es;
+    const cuuint64_t dims[4] = {(cuuint64_t)L->nx, (cuuint64_t)L->ny, (cuuint64_t)L->nz, (cuuint64_t)L->planes.size()};
+    const cuuint64_t strides[3] = {(cuuint64_t)L->nx * es, (cuuint64_t)(L->nx * L->ny) * es,
+                                   (cuuint64_t)L->plane * es};
+    const cuuint32_t box[4] = {(cuuint32_t)box_x, (cuuint32_t)kTmaRows, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(&L->tmap, dt, 4, L->base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    L->tma_ok = (r == CUDA_SUCCESS) && L->origin == kTmaOrigin;
+}
+
+// Tensor-map plane of each current population array.
+void plane_indices(const bgk_lattice* L, int* pa) {
+    for (int d = 0; d < 19; ++d)
+        pa[d] = (int)(((char*)L->a[d] - L->base) / ((long long)L->plane * L->es));
+}
+
+int tma_step(bgk_lattice* L, cudaStream_t st) {
+    int pa[19];
+    plane_indices(L, pa);
+    KIND_DISPATCH(L->p.kind, (launch_sweep_tma<S, C>(&L->p, L->a, L->b, &L->tmap, pa, L->err, st)));
 }
 
 }  // namespace
@@ -193,8 +266,37 @@ int bgk_lattice_create(const bgk_lattice_desc* d, bgk_lattice** out) {
     } else {
         for (int q = 0; q < 19; ++q) L->b[q] = L->a[q];
     }
+    e = cudaMalloc(&L->err, sizeof(int));
+    if (e != cudaSuccess) {
+        cudaFree(L->base);
+        delete L;
+        return set_error(BGK_ERR_NOMEM, "status flag: %s", cudaGetErrorString(e));
+    }
+    cudaMemset(L->err, 0, sizeof(int));
+    make_tensor_map(L);
     *out = L;
     return BGK_OK;
+}
+
+int bgk_lattice_status(const bgk_lattice* L) {
+    if (!L) return set_error(BGK_ERR_ARG, "null lattice");
+    int flag = 0;
+    const cudaError_t e = cudaMemcpy(&flag, L->err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "status: %s", cudaGetErrorString(e));
+    if (flag) return set_error(BGK_ERR_CUDA, "a TMA sweep gave up waiting for its copies; the state is undefined");
+    return BGK_OK;
+}
+
+int bgk_lattice_uses_tma(const bgk_lattice* L) {
+    if (!L) return 0;
+    const bool has_obs = L->p.obs && L->p.imin <= L->p.imax;
+    return (L->tma_ok && g_tma_kernels && !has_obs) ? 1 : 0;
+}
+
+int bgk_set_tma_kernels(int enable) {
+    const int prev = g_tma_kernels ? 1 : 0;
+    g_tma_kernels = enable != 0;
+    return prev;
 }
 
 int bgk_lattice_destroy(bgk_lattice* L) {
@@ -205,6 +307,7 @@ int bgk_lattice_destroy(bgk_lattice* L) {
     if (L->obs_dev) cudaFree(L->obs_dev);
     if (L->ws) cudaFree(L->ws);
     if (L->mom) cudaFree(L->mom);
+    if (L->err) cudaFree(L->err);
     delete L;
     return BGK_OK;
 }

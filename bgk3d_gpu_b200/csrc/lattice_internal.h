@@ -1,6 +1,7 @@
 // Definition of the library-owned lattice object, shared by lattice.cu and
 // the batched stepper (batch.cu).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <vector>
 #include "bgk3d_b200.h"
@@ -25,6 +26,9 @@ struct bgk_lattice {
     int graph_steps = 0;
     double* mom = nullptr;       // per-block partial moments of fused steps
     size_t mom_bytes = 0;
+    alignas(64) CUtensorMap tmap; // the allocation as x, y, z, plane (sweep_tma.cuh)
+    bool tma_ok = false;         // tmap is valid (AB pattern, driver support)
+    int* err = nullptr;          // device flag set by a TMA kernel wait that gave up
 };
 
 // Shared by the lattice's host-transfer paths (lattice.cu, lattice_io.cu).

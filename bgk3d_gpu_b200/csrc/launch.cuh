@@ -1,12 +1,14 @@
 // Launch wrappers (templates) of every kernel, instantiated once per storage
 // kind by the inst_*.cu translation units; declared in kernels.h.
 #pragma once
+#include <algorithm>
 #include <cuda_runtime.h>
 #include "bgk3d_b200.h"
 #include "bgk_internal.h"
 #include "host_args.cuh"
 #include "sweep_ab.cuh"
 #include "sweep_aa.cuh"
+#include "sweep_tma.cuh"
 #include "reduce.cuh"
 #include "batch.cuh"
 #include "init.cuh"
@@ -97,6 +99,82 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
         case BC_INFLOW: by_variant<AbLaunch, S, C, BC_INFLOW>(nelem, cm, obs, A, nb, st); break;
     }
     return check_launch("sweep_ab_kernel");
+}
+
+// TMA-staged sweep (sweep_tma.cuh) for library-owned AB lattices without
+// obstacle; map is the lattice's tensor map, pa[d] the plane of a[d].
+
+template <class S, class C, int BC, int CM>
+int launch_tma_variant(const SweepArgs<S, C>& A, const TmaSched& T, const CUtensorMap& map, cudaStream_t st) {
+    auto kern = sweep_tma_kernel<S, C, BC, CM>;
+    const size_t smem = TmaBox<S>::SMEM;
+    static int grid_per_sm = 0;   // per instantiation, set up on the first launch
+    if (grid_per_sm == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "tma smem attribute: %s", cudaGetErrorString(e));
+        int per = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kTmaThreads, smem);
+        if (e != cudaSuccess || per < 1) return set_error(BGK_ERR_CUDA, "tma occupancy: %s", cudaGetErrorString(e));
+        grid_per_sm = per;
+    }
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long grid = std::min<long long>((long long)nsm * grid_per_sm, (long long)T.ntiles);
+    kern<<<(unsigned)std::max<long long>(grid, 1), kTmaThreads, smem, st>>>(A, T, map);
+    if (int e = check_launch("sweep_tma_kernel")) return e;
+    const long long l = A.l, m = A.m, n = A.n;
+    const long long faces = (n > 1 ? 2 : 1) * l * m + (m > 1 ? 2 : 1) * l * std::max(n - 2, 0LL) +
+                            (l > 1 ? 2 : 1) * std::max(m - 2, 0LL) * std::max(n - 2, 0LL);
+    sweep_faces_kernel<S, C, BC, CM><<<(unsigned)((faces + 255) / 256), 256, 0, st>>>(A);
+    return check_launch("sweep_faces_kernel");
+}
+
+template <class S, class C, int BC>
+int launch_tma_bc(const SweepArgs<S, C>& A, const TmaSched& T, const CUtensorMap& map, int cm, cudaStream_t st) {
+    switch (cm) {
+        case CM_STRICT: return launch_tma_variant<S, C, BC, CM_STRICT>(A, T, map, st);
+        case CM_STRICT_GENERIC: return launch_tma_variant<S, C, BC, CM_STRICT_GENERIC>(A, T, map, st);
+        case CM_FAST:
+            if constexpr (sizeof(C) == 4) return launch_tma_variant<S, C, BC, CM_FAST>(A, T, map, st);
+            break;
+        default:
+            if constexpr (sizeof(C) == 4) return launch_tma_variant<S, C, BC, CM_FAST_GENERIC>(A, T, map, st);
+            break;
+    }
+    return set_error(BGK_ERR_ARG, "collision mode %d", cm);
+}
+
+template <class S, class C>
+int launch_sweep_tma(const bgk_sweep_params* p, void* const* a, void* const* b, const void* tmap, const int* pa,
+                     int* err, cudaStream_t st) {
+    if constexpr (sizeof(C) != 4 || sizeof(S) > 4) {
+        return set_error(BGK_ERR_UNSUPPORTED, "the TMA sweep serves float compute");
+    } else {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
+    segment_geometry(A, a[0]);
+    A.mom = nullptr;
+    if (p->bcase == BC_INFLOW) {
+        dim3 blk(128), grd((p->m + 127) / 128, p->n);
+        outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
+        if (int e = check_launch("outflow_halo_kernel")) return e;
+    }
+    TmaSched T;
+    for (int d = 0; d < 19; ++d) T.pa[d] = pa[d];
+    T.ntx = (p->l + 63) / 64;
+    T.nty = (p->m + kTmaRows - 1) / kTmaRows;
+    T.ntiles = (uint32_t)((long long)T.ntx * T.nty * p->n);
+    T.err = err;
+    const CUtensorMap& map = *static_cast<const CUtensorMap*>(tmap);
+    const int cm = coll_mode(A);
+    switch (p->bcase) {
+        case BC_DRIVEN: return launch_tma_bc<S, C, BC_DRIVEN>(A, T, map, cm, st);
+        case BC_PERIODIC: return launch_tma_bc<S, C, BC_PERIODIC>(A, T, map, cm, st);
+        case BC_CHANNEL: return launch_tma_bc<S, C, BC_CHANNEL>(A, T, map, cm, st);
+        case BC_INFLOW: return launch_tma_bc<S, C, BC_INFLOW>(A, T, map, cm, st);
+        default: return set_error(BGK_ERR_ARG, "the TMA sweep needs a boundary case");
+    }
+    }
 }
 
 template <class S, class C>
@@ -230,6 +308,8 @@ int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n,
     namespace bgk {                                                                                \
     template int launch_sweep<S, C>(const bgk_sweep_params*, void* const*, void* const*, double*,  \
                                     cudaStream_t);                                                 \
+    template int launch_sweep_tma<S, C>(const bgk_sweep_params*, void* const*, void* const*,        \
+                                        const void*, const int*, int*, cudaStream_t);              \
     }
 #define BGK_INSTANTIATE_AA(S, C)                                                                   \
     namespace bgk {                                                                                \

@@ -151,8 +151,32 @@ __device__ __forceinline__ uint32_t obstacle_links(const SweepArgs<S, C>& P, int
 // CM: collision mode; OBS: the lattice may have an obstacle (P.obs is then
 // tested at run time; OBS = false compiles the obstacle logic out).
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
+__device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j, int k, double (&m5)[5]);
+
+// Collision of the gathered values x[] (storage units) of the node at element
+// c, the store of the new populations (b[0..17], pop 19 in place) and, with
+// P.mom, the node's moments of the stored state.
+template <class S, class C, class IDX, int CM>
+__device__ __forceinline__ void collide_store(const SweepArgs<S, C>& P, const C (&x)[19], IDX c, double (&m5)[5]) {
+    const float inv = P.inv_scale;
+    C y[19];
+    collide_cm<S, C, CM>(x, y, P.col, P.fc, inv);
+    S sv[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) sv[d] = Conv<S, C>::pack(y[d]);
+#pragma unroll
+    for (int d = 0; d < 18; ++d) P.b[d][c] = sv[d];
+    const_cast<S*>(P.a[18])[c] = sv[18];
+    if (P.mom != nullptr) {
+        C s[19];
+#pragma unroll
+        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(sv[d], inv);
+        diagno_node<C>(s, P.col.cte1, m5);
+    }
+}
+
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
-    typedef Faces<BC> F;
     const int lane = threadIdx.x & 31;
     const uint32_t row = P.div_seg.div(gw);
     if (row >= P.nrows) return;
@@ -165,13 +189,22 @@ __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw
     const int sh = (int)((P.align_base + (long long)rowoff + 1) & 31);
     const int i = seg * 32 + lane + 1 - (P.nseg_aligned ? 0 : sh);
     if (i < 1 || i > P.l) return;
-    const IDX c = rowoff + (IDX)i;
+    sweep_at<S, C, BC, IDX, CM, OBS>(P, i, j, k, m5);
+}
+
+// The 19 pulled values (storage units) of interior node (i, j, k), 1 <= i <= l
+// etc., with every boundary link resolved; false for a solid node.
+template <class S, class C, int BC, class IDX, bool OBS>
+__device__ __forceinline__ bool gather_at(const SweepArgs<S, C>& P, int i, int j, int k, C (&x)[19]) {
+    typedef Faces<BC> F;
+    const IDX nx = (IDX)P.nx, nxy = (IDX)P.nxy;
+    const IDX c = nx * (IDX)j + nxy * (IDX)k + (IDX)i;
 
     uint32_t sl = 0;
     if (OBS && P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
         j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1) {
         sl = obstacle_links(P, i, j, k);
-        if (sl & 0x80000000u) return;   // solid node: not updated
+        if (sl & 0x80000000u) return false;   // solid node: not updated
     }
     // source offsets for c = +1 (source at -1) and c = -1 (source at +1) on
     // each axis; periodic axes wrap, others step into the halo (those links
@@ -185,8 +218,6 @@ __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw
     const bool wxm = F::WX && i == 1, wxp = F::WX && i == P.l;
     const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
     const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
-    const float inv = P.inv_scale;
-    C x[19];
 #pragma unroll
     for (int d = 0; d < 18; ++d) {
         const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
@@ -207,20 +238,16 @@ __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw
         x[d] = v;
     }
     x[18] = Conv<S, C>::raw(P.a[18][c]);
-    C y[19];
-    collide_cm<S, C, CM>(x, y, P.col, P.fc, inv);
-    S sv[19];
-#pragma unroll
-    for (int d = 0; d < 19; ++d) sv[d] = Conv<S, C>::pack(y[d]);
-#pragma unroll
-    for (int d = 0; d < 18; ++d) P.b[d][c] = sv[d];
-    const_cast<S*>(P.a[18])[c] = sv[18];
-    if (P.mom != nullptr) {
-        C s[19];
-#pragma unroll
-        for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(sv[d], inv);
-        diagno_node<C>(s, P.col.cte1, m5);
-    }
+    return true;
+}
+
+// The time step of interior node (i, j, k): gather, collision, store and
+// (with P.mom) the node's moments.
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
+__device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j, int k, double (&m5)[5]) {
+    C x[19];
+    if (!gather_at<S, C, BC, IDX, OBS>(P, i, j, k, x)) return;
+    collide_store<S, C, IDX, CM>(P, x, (IDX)P.nx * (IDX)j + (IDX)P.nxy * (IDX)k + (IDX)i, m5);
 }
 
 // One launch = one time step.  With P.mom set, every block also writes the
