@@ -72,6 +72,12 @@ def bind(L) -> None:
     L.bgk_set_tma_kernels.restype = c_int
     L.bgk_lattice_status.argtypes = [c_void_p]
     L.bgk_lattice_status.restype = c_int
+    L.bgk_lattice_set_sphere.argtypes = [c_void_p, c_double, c_double, c_double, c_double]
+    L.bgk_lattice_set_sphere.restype = c_int
+    L.bgk_set_retained_bytes.argtypes = [c_size_t]
+    L.bgk_set_retained_bytes.restype = c_int
+    L.bgk_trim_memory.argtypes = []
+    L.bgk_trim_memory.restype = c_int
     L.bgk_lattice_init.argtypes = [c_void_p, c_int, c_void_p, c_void_p]
     L.bgk_lattice_init.restype = c_int
     L.bgk_lattice_load.argtypes = [c_void_p, c_void_p, c_void_p]

@@ -90,8 +90,8 @@ def run_case(case: dict, kind: str, steps: int, every: int, pattern: str = "ab")
     wall = time.perf_counter() - t0
     rho, u = velocity_field(lat, scale)
     fluid = None
-    if c.get("obstacle") is not None:
-        fluid = torch.from_numpy(c["obstacle"] != 1).to(lat.device)
+    if CS.obstacle_mask(c) is not None:
+        fluid = torch.from_numpy(CS.obstacle_mask(c) != 1).to(lat.device)
     lat.close()
     return {"kind": kind, "series": series, "u": u, "rho": rho, "fluid": fluid, "wall_s": wall,
             "glups_incl_diag": nodes * steps / wall / 1e9}

@@ -28,7 +28,7 @@ NVCC_FLAGS = ARCH + [
     "-I" + INCLUDE, "-I" + CSRC,
 ]
 
-LIB_SOURCES = ["bgk_api.cu", "lattice.cu", "lattice_io.cu", "diag.cu", "batch.cu", "noalloc.cu"] + [
+LIB_SOURCES = ["bgk_api.cu", "lattice.cu", "lattice_io.cu", "diag.cu", "batch.cu", "noalloc.cu", "devmem.cu"] + [
     f"inst_{kind}_{group}.cu" for kind in ("f64", "f32", "f16", "bf16", "f32f64") for group in ("ab", "aa", "batch", "misc")]
 LIB = "libbgk3d_b200.so"
 DROPIN_SP = "libbgk3d_dropin_sp.so"

@@ -5,8 +5,10 @@ reference's own obstacle builder (SRC/build.obs.F90) and collision
 parameters (SRC/hencol.F90).
 
 A case is a dict of Lattice keyword arguments plus `init` (a function that
-returns rho, ux, uy, uz device fields [k, j, i]) and, for obstacle flows,
-`obstacle` (int32 mask [k, j, i]) and `drag_box`.
+returns rho, ux, uy, uz device fields [k, j, i]), `flow` (the on-device
+initial condition) and, for obstacle flows, `sphere` (centre, radius^2: the
+mask is built on the device; obstacle_mask() builds it on the host) or
+`obstacle` (int32 mask [k, j, i]), and `drag_box`.
 """
 from __future__ import annotations
 
@@ -55,6 +57,40 @@ def solid_sphere_obstacle(l: int, m: int, n: int, diameter: float, center):
     d2 = (i - center[0]) ** 2 + (j - center[1]) ** 2 + (k - center[2]) ** 2
     obs = (d2 <= r2).astype(np.int32)
     return obs, _bbox(obs)
+
+
+def sphere_bbox(l: int, m: int, n: int, diameter: float, center):
+    """Bounding box (imin, imax, jmin, jmax, kmin, kmax) of the solid nodes of
+    solid_sphere_obstacle, from the extents and the rule alone (no mask)."""
+    r2 = (diameter / 2.0) ** 2
+    ext = (l, m, n)
+
+    def near(a, c):   # smallest (x - c)^2 over the integers 1..a
+        x = min(max(int(round(c)), 1), a)
+        return (x - c) ** 2
+
+    lo, hi = [], []
+    for ax in range(3):
+        others = sum(near(ext[b], center[b]) for b in range(3) if b != ax)
+        xs = [x for x in range(1, ext[ax] + 1) if (x - center[ax]) ** 2 + others <= r2]
+        if not xs:
+            return None
+        lo.append(min(xs))
+        hi.append(max(xs))
+    return (lo[0], hi[0], lo[1], hi[1], lo[2], hi[2])
+
+
+def obstacle_mask(case: dict):
+    """The case's int32 obstacle mask [k, j, i] (built on the host), or None."""
+    if case.get("obstacle") is not None:
+        return case["obstacle"]
+    if case.get("sphere") is not None:
+        center, r2 = case["sphere"]
+        k, j, i = np.meshgrid(np.arange(1, case["n"] + 1), np.arange(1, case["m"] + 1),
+                              np.arange(1, case["l"] + 1), indexing="ij")
+        d2 = (i - center[0]) ** 2 + (j - center[1]) ** 2 + (k - center[2]) ** 2
+        return (d2 <= r2).astype(np.int32)
+    return None
 
 
 def _bbox(obs):
@@ -124,10 +160,11 @@ def sphere(l: int = 512, m: int = 256, n: int = 256, kind: str = "f32", diameter
     x = l+1 (equilibrium at rho = 1 with the momentum of node l, the
     reference's rule), periodic y/z, nu = u_in D / Re, rest initial state."""
     nu = u_in * diameter / re
-    obs, bbox = solid_sphere_obstacle(l, m, n, diameter, center)
+    bbox = sphere_bbox(l, m, n, diameter, center)
     return dict(l=l, m=m, n=n, kind=kind, bcase="inflow", omega=1.0 / tau_from_nu(nu), u_inflow=u_in,
-                init=_rest(l, m, n), flow=("rest", (1.0, 0.0, 0.0, 0.0)), obstacle=obs,
-                drag_box=drag_box(bbox), radius=diameter / 2.0, nu=nu, name=f"sphere{l}x{m}x{n}_{kind}", **kw)
+                init=_rest(l, m, n), flow=("rest", (1.0, 0.0, 0.0, 0.0)),
+                sphere=(tuple(float(v) for v in center), (diameter / 2.0) ** 2),
+                drag_box=drag_box(bbox) if bbox else None, radius=diameter / 2.0, nu=nu, name=f"sphere{l}x{m}x{n}_{kind}", **kw)
 
 
 LATTICE_KEYS = ("kind", "bcase", "omega", "lid_force", "u_inflow", "force_mode", "force", "scale",
@@ -150,7 +187,9 @@ def make_lattice(case: dict, pattern: str = "ab", scale: float | None = None, on
     elif kw.get("kind") == "f16":
         kw["scale"] = 256.0
     lat = Lattice(case["l"], case["m"], case["n"], **kw)
-    if case.get("obstacle") is not None:
+    if case.get("sphere") is not None:
+        lat.set_sphere(*case["sphere"])          # mask built on the device
+    elif case.get("obstacle") is not None:
         lat.set_obstacle(case["obstacle"])
     if on_device and case.get("flow") is not None:
         lat.init_flow(*case["flow"])

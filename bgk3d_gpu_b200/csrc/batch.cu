@@ -198,14 +198,15 @@ int bgk_batch_create(bgk_lattice* const* lats, int count, bgk_batch** out) {
     B->ntiles = begin[count];
     for (int i = 0; i < count; ++i) B->expect.push_back(lats[i]->steps);
     record_base(B);
-    cudaError_t e = cudaMalloc(&B->desc, host.size());
-    if (e == cudaSuccess) e = cudaMalloc(&B->tile_begin, begin.size() * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&B->counter, 2 * sizeof(unsigned));
-    if (e != cudaSuccess) { bgk_batch_destroy(B); return set_error(BGK_ERR_NOMEM, "batch tables: %s", cudaGetErrorString(e)); }
-    cudaMemcpy(B->desc, host.data(), host.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(B->tile_begin, begin.data(), begin.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
-    cudaMemset(B->counter, 0, 2 * sizeof(unsigned));
-    e = cudaDeviceSynchronize();
+    int rc = dev_alloc(reinterpret_cast<void**>(&B->desc), host.size(), false, "batch descriptors");
+    if (!rc) rc = dev_alloc(reinterpret_cast<void**>(&B->tile_begin), begin.size() * sizeof(uint32_t), false, "tile table");
+    if (!rc) rc = dev_alloc(reinterpret_cast<void**>(&B->counter), 2 * sizeof(unsigned), true, "tile counter");
+    if (rc) { bgk_batch_destroy(B); return rc; }
+    cudaStream_t s = setup_stream();
+    cudaError_t e = cudaMemcpyAsync(B->desc, host.data(), host.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(B->tile_begin, begin.data(), begin.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { bgk_batch_destroy(B); return set_error(BGK_ERR_CUDA, "batch tables: %s", cudaGetErrorString(e)); }
     *out = B;
     return BGK_OK;
@@ -235,9 +236,9 @@ int bgk_batch_destroy(bgk_batch* B) {
     if (!B) return BGK_OK;
     drop_graph(B);
     if (B->cap) cudaStreamDestroy(B->cap);
-    if (B->desc) cudaFree(B->desc);
-    if (B->tile_begin) cudaFree(B->tile_begin);
-    if (B->counter) cudaFree(B->counter);
+    dev_free(B->desc);
+    dev_free(B->tile_begin);
+    dev_free(B->counter);
     delete B;
     return BGK_OK;
 }

@@ -33,6 +33,13 @@ int sweep_launch_mom(const struct bgk_sweep_params* p, void* const* a, void* con
 long long sweep_blocks(const struct bgk_sweep_params* p, const void* a0);
 // Second pass over nparts partials of 5 doubles into out[0..4].
 int finalize_moments(const double* partials, long long nparts, double* out, cudaStream_t st);
+// Device memory of library-owned objects from the per-device pool
+// (zeroed when asked), ready for any stream on return; dev_free waits for
+// the device, as cudaFree does, and returns the block to the pool.
+int dev_alloc(void** p, size_t bytes, bool zero, const char* what);
+void dev_free(void* p);
+// Private non-blocking stream for set-up kernels and copies.
+cudaStream_t setup_stream();
 // The two launches of the FP64 drag/lift reduction.
 int draglift_launch(const struct bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
                     int ke, double* out, double* ws, size_t ws_bytes, cudaStream_t st);

@@ -119,12 +119,29 @@ int ensure_workspace(const bgk_lattice* Lc) {
     bgk_lattice* L = const_cast<bgk_lattice*>(Lc);
     const size_t need = std::max<size_t>(bgk_reduce_workspace_bytes(L->desc.l, L->desc.m, L->desc.n), 1 << 16);
     if (L->ws && L->ws_bytes >= need) return BGK_OK;
-    if (L->ws) cudaFree(L->ws);
+    dev_free(L->ws);
     L->ws = nullptr;
-    cudaError_t e = cudaMalloc(&L->ws, need);
-    if (e != cudaSuccess) return set_error(BGK_ERR_NOMEM, "workspace: %s", cudaGetErrorString(e));
+    if (int rc = dev_alloc(reinterpret_cast<void**>(&L->ws), need, false, "workspace")) return rc;
     L->ws_bytes = need;
     return BGK_OK;
+}
+
+// Solid sphere mask on the device: obs[(i-1) + l (j-1) + l m (k-1)] = 1 where
+// (i - cx)^2 + (j - cy)^2 + (k - cz)^2 <= r2, with the bounding box of the
+// solid nodes gathered by atomics into box[0..5] (min i, max i, min j, ...).
+__global__ void sphere_mask_kernel(int32_t* obs, int l, int m, int n, double cx, double cy, double cz, double r2,
+                                   int* box) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)l * m * n) return;
+    const int i = (int)(t % l) + 1, j = (int)((t / l) % m) + 1, k = (int)(t / ((long long)l * m)) + 1;
+    const double dx = i - cx, dy = j - cy, dz = k - cz;
+    const int solid = (dx * dx + dy * dy + dz * dz <= r2) ? 1 : 0;
+    obs[t] = solid;
+    if (solid) {
+        atomicMin(&box[0], i); atomicMax(&box[1], i);
+        atomicMin(&box[2], j); atomicMax(&box[3], j);
+        atomicMin(&box[4], k); atomicMax(&box[5], k);
+    }
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -249,13 +266,10 @@ int bgk_lattice_create(const bgk_lattice_desc* d, bgk_lattice** out) {
     L->p.fast = d->fast;
     if (int e = validate(&L->p)) { delete L; return e; }
     L->bytes = bgk_lattice_device_bytes(d);
-    cudaError_t e = cudaMalloc(&L->base, L->bytes);
-    if (e != cudaSuccess) {
+    if (int rc = dev_alloc(reinterpret_cast<void**>(&L->base), L->bytes, true, "lattice")) {
         delete L;
-        return set_error(BGK_ERR_NOMEM, "lattice of %zu bytes: %s", (size_t)bgk_lattice_device_bytes(d),
-                         cudaGetErrorString(e));
+        return rc;
     }
-    cudaMemset(L->base, 0, L->bytes);
     const int np = nplanes(d);
     L->planes.resize(np);
     for (int q = 0; q < np; ++q) L->planes[q] = L->base + ((size_t)q * L->plane + L->origin) * L->es;
@@ -266,13 +280,11 @@ int bgk_lattice_create(const bgk_lattice_desc* d, bgk_lattice** out) {
     } else {
         for (int q = 0; q < 19; ++q) L->b[q] = L->a[q];
     }
-    e = cudaMalloc(&L->err, sizeof(int));
-    if (e != cudaSuccess) {
-        cudaFree(L->base);
+    if (int rc = dev_alloc(reinterpret_cast<void**>(&L->err), sizeof(int), true, "status flag")) {
+        dev_free(L->base);
         delete L;
-        return set_error(BGK_ERR_NOMEM, "status flag: %s", cudaGetErrorString(e));
+        return rc;
     }
-    cudaMemset(L->err, 0, sizeof(int));
     make_tensor_map(L);
     *out = L;
     return BGK_OK;
@@ -303,19 +315,55 @@ int bgk_lattice_destroy(bgk_lattice* L) {
     if (!L) return BGK_OK;
     drop_graph(L);
     if (L->cap_stream) cudaStreamDestroy(L->cap_stream);
-    if (L->base) cudaFree(L->base);
-    if (L->obs_dev) cudaFree(L->obs_dev);
-    if (L->ws) cudaFree(L->ws);
-    if (L->mom) cudaFree(L->mom);
-    if (L->err) cudaFree(L->err);
+    dev_free(L->base);
+    dev_free(L->obs_dev);
+    dev_free(L->ws);
+    dev_free(L->mom);
+    dev_free(L->err);
     delete L;
+    return BGK_OK;
+}
+
+int bgk_lattice_set_sphere(bgk_lattice* L, double cx, double cy, double cz, double r2) {
+    if (!L) return set_error(BGK_ERR_ARG, "null lattice");
+    drop_graph(L);
+    dev_free(L->obs_dev);
+    L->obs_dev = nullptr;
+    L->p.obs = nullptr;
+    L->p.imin = 1; L->p.imax = 0; L->p.jmin = 1; L->p.jmax = 0; L->p.kmin = 1; L->p.kmax = 0;
+    const int l = L->desc.l, m = L->desc.m, n = L->desc.n;
+    const long long nodes = (long long)l * m * n;
+    int32_t* obs = nullptr;
+    int* box = nullptr;
+    if (int rc = dev_alloc(reinterpret_cast<void**>(&obs), (size_t)nodes * sizeof(int32_t), false, "obstacle mask"))
+        return rc;
+    if (int rc = dev_alloc(reinterpret_cast<void**>(&box), 6 * sizeof(int), false, "bbox")) { dev_free(obs); return rc; }
+    int hb[6] = {l + 1, 0, m + 1, 0, n + 1, 0};
+    cudaStream_t s = setup_stream();
+    cudaError_t e = cudaMemcpyAsync(box, hb, sizeof hb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        sphere_mask_kernel<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(obs, l, m, n, cx, cy, cz, r2, box);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hb, box, sizeof hb, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    dev_free(box);
+    if (e != cudaSuccess) { dev_free(obs); return set_error(BGK_ERR_CUDA, "sphere mask: %s", cudaGetErrorString(e)); }
+    if (hb[1] == 0) { dev_free(obs); return BGK_OK; }   // no solid node
+    bgk_sweep_params q = L->p;
+    q.obs = obs; q.obs_nx = l; q.obs_ny = m;
+    q.imin = hb[0]; q.imax = hb[1]; q.jmin = hb[2]; q.jmax = hb[3]; q.kmin = hb[4]; q.kmax = hb[5];
+    if (int err = validate(&q)) { dev_free(obs); return err; }
+    L->obs_dev = obs;
+    L->p = q;
     return BGK_OK;
 }
 
 int bgk_lattice_set_obstacle(bgk_lattice* L, const int32_t* obs) {
     if (!L) return set_error(BGK_ERR_ARG, "null lattice");
     drop_graph(L);
-    if (L->obs_dev) { cudaFree(L->obs_dev); L->obs_dev = nullptr; }
+    dev_free(L->obs_dev);
+    L->obs_dev = nullptr;
     L->p.obs = nullptr;
     L->p.imin = 1; L->p.imax = 0; L->p.jmin = 1; L->p.jmax = 0; L->p.kmin = 1; L->p.kmax = 0;
     if (!obs) return BGK_OK;
@@ -335,10 +383,15 @@ int bgk_lattice_set_obstacle(bgk_lattice* L, const int32_t* obs) {
     q.imin = b[0]; q.imax = b[1]; q.jmin = b[2]; q.jmax = b[3]; q.kmin = b[4]; q.kmax = b[5];
     if (int e = validate(&q)) return e;
     const size_t nb = (size_t)l * m * n * sizeof(int32_t);
-    cudaError_t e = cudaMalloc(&L->obs_dev, nb);
-    if (e != cudaSuccess) return set_error(BGK_ERR_NOMEM, "obstacle mask: %s", cudaGetErrorString(e));
-    e = cudaMemcpy(L->obs_dev, obs, nb, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "obstacle copy: %s", cudaGetErrorString(e));
+    if (int rc = dev_alloc(reinterpret_cast<void**>(&L->obs_dev), nb, false, "obstacle mask")) return rc;
+    cudaStream_t s = setup_stream();
+    cudaError_t e = cudaMemcpyAsync(L->obs_dev, obs, nb, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        dev_free(L->obs_dev);
+        L->obs_dev = nullptr;
+        return set_error(BGK_ERR_CUDA, "obstacle copy: %s", cudaGetErrorString(e));
+    }
     q.obs = L->obs_dev;
     L->p = q;
     return BGK_OK;
@@ -428,10 +481,9 @@ int bgk_lattice_step_moments(bgk_lattice* L, int nsteps, int every, double* out_
     const long long nb = sweep_blocks(&L->p, L->a[0]);
     const size_t need = (size_t)nb * 5 * sizeof(double);
     if (L->mom_bytes < need) {
-        if (L->mom) cudaFree(L->mom);
+        dev_free(L->mom);
         L->mom = nullptr; L->mom_bytes = 0;
-        cudaError_t e = cudaMalloc(&L->mom, need);
-        if (e != cudaSuccess) return set_error(BGK_ERR_NOMEM, "moment partials: %s", cudaGetErrorString(e));
+        if (int rc = dev_alloc(reinterpret_cast<void**>(&L->mom), need, false, "moment partials")) return rc;
         L->mom_bytes = need;
     }
     const int samples = nsteps / every;

@@ -207,6 +207,11 @@ class Lattice:
         o = np.ascontiguousarray(obs, np.int32)
         check(self.L.bgk_lattice_set_obstacle(self.h, o.ctypes.data), "set_obstacle")
 
+    def set_sphere(self, center, r2: float) -> None:
+        """Solid sphere obstacle built on the device (bgk_lattice_set_sphere)."""
+        check(self.L.bgk_lattice_set_sphere(self.h, float(center[0]), float(center[1]), float(center[2]),
+                                            float(r2)), "bgk_lattice_set_sphere")
+
     def upload(self, state: np.ndarray) -> None:
         st = np.ascontiguousarray(state)
         check(self.L.bgk_lattice_load(self.h, st.ctypes.data, self._stream()), "bgk_lattice_load")
@@ -343,6 +348,16 @@ class Batch:
     @property
     def nodes(self) -> int:
         return int(self.L.bgk_batch_nodes(self.h))
+
+
+def set_retained_bytes(nbytes: int) -> None:
+    """Bytes of freed lattice memory the current device's pool keeps for reuse
+    (bgk_set_retained_bytes; 0, the default, gives it back at once)."""
+    check(lib().bgk_set_retained_bytes(int(nbytes)), "bgk_set_retained_bytes")
+
+
+def trim_memory() -> None:
+    check(lib().bgk_trim_memory(), "bgk_trim_memory")
 
 
 def save_name(itime: int) -> str:

@@ -6,8 +6,11 @@ requests as soon as memory frees up (admission by the device bytes each
 lattice needs, against a budget), and advances resident solves in rounds:
 each round steps a set of lattices by the same number of steps -- the
 smallest remaining step count in the set, capped -- with one batched launch
-per storage kind (bgk3d_batch.h), so a request that arrives while others are
-running starts at the next round and its work overlaps theirs.  A solve
+per storage kind (bgk3d_batch.h) for the small lattices and the lattice's
+own step graph for those that fill the GPU alone, so a request that arrives
+while others are running starts at the next round and its work overlaps
+theirs.  Lattice memory comes from the library's pool, which keeps freed
+blocks for the next request (bgk_set_retained_bytes).  A solve
 leaves as soon as its steps are done; its result is the FP64 moments (and,
 for the sphere, drag/lift) of its final state.
 
@@ -18,7 +21,10 @@ Round policies (`mode`):
               rest wait.  Short solves finish early instead of sharing the
               GPU with long ones, and the batch still saturates the device.
   shared      every resident solve in every round (processor sharing).
-  fifo        one solve at a time, in arrival order.
+  fifo        one solve at a time, in arrival order (batched launches of one).
+  plain       one solve at a time, in arrival order, each advanced by
+              Lattice.step alone: the sequential plain launches that the
+              batched modes are compared with.
 
 Because the batched kernel is bit-identical to stepping a lattice alone, a
 request's result does not depend on what it was batched with (tested).
@@ -38,7 +44,7 @@ import numpy as np
 import torch
 
 from . import cases as CS
-from .lattice import Batch
+from .lattice import Batch, set_retained_bytes
 
 
 @dataclasses.dataclass
@@ -81,16 +87,23 @@ def case_of(req: Request) -> dict:
     return c
 
 
+def extents(req: Request):
+    """(l, m, n, bcase) of a request's lattice, without building its case."""
+    s = req.side
+    if req.case == "sphere":
+        return 2 * s, s, s, "inflow"
+    return s, s, s, {"ldc": "driven", "tgv": "periodic"}[req.case]
+
+
 def lattice_bytes(req: Request) -> int:
     from .lattice import lib
     from ._lattice_abi import LatticeDesc
     import ctypes
-    c = case_of(req)
+    l, m, n, bcase = extents(req)
     d = LatticeDesc()
     kind = {"f32": 1, "f16": 2}[req.kind]
     lib().bgk_lattice_desc_init(ctypes.byref(d), kind, {"driven": 0, "periodic": 1, "channel": 2,
-                                                       "inflow": 3}[c["bcase"]], c["l"], c["m"], c["n"],
-                                c["omega"])
+                                                       "inflow": 3}[bcase], l, m, n, 1.0 / req.tau)
     return int(lib().bgk_lattice_device_bytes(ctypes.byref(d)))
 
 
@@ -113,11 +126,16 @@ class _Active:
 
 
 class Server:
-    def __init__(self, budget_bytes: float = 150e9, max_chunk: int = 200, floor_nodes: float = 8e6):
+    def __init__(self, budget_bytes: float = 150e9, max_chunk: int = 200, floor_nodes: float = 8e6,
+                 alone_nodes: float = 2e6):
         free, _ = torch.cuda.mem_get_info()
         self.budget = min(budget_bytes, free * 0.92)
         self.max_chunk = max_chunk
         self.floor_nodes = floor_nodes
+        # a lattice this large fills the GPU by itself: it steps with its own
+        # graph in the round instead of joining the tile-queue batch, whose
+        # tile lookup costs a few per cent at this size
+        self.alone_nodes = alone_nodes
 
     def select(self, active, mode: str):
         """The solves stepped this round (see the module docstring)."""
@@ -133,81 +151,103 @@ class Server:
 
     def run(self, trace, mode: str = "continuous", keep_states: bool = False):
         """Serve the trace; returns (per-request records, summary)."""
-        if mode not in ("continuous", "shared", "fifo"):
+        if mode not in ("continuous", "shared", "fifo", "plain"):
             raise ValueError(f"unknown mode {mode!r}")
+        one_at_a_time = mode in ("fifo", "plain")
         pending = sorted(trace, key=lambda r: r.arrival)
         active: list[_Active] = []
         done = []
         used = 0
         lups = 0
         batches: dict = {}          # kind -> (member ids, Batch)
+        set_retained_bytes(int(self.budget))    # lattice memory is reused, not mapped anew
         t0 = time.perf_counter()
         rounds = 0
+        t_admit = t_wait = 0.0
 
-        def drop_batches():
-            for _, b in batches.values():
-                b.close()
-            batches.clear()
-
-        while pending or active:
-            now = time.perf_counter() - t0
-            # admission: arrived requests, in arrival order, while memory allows
+        def admit(now):
+            nonlocal used, t_admit
+            ta = time.perf_counter()
             while pending and pending[0].arrival <= now:
                 need = lattice_bytes(pending[0])
                 if need > self.budget:
                     raise RuntimeError(f"request {pending[0].rid} needs {need} bytes, more than the budget")
-                if (mode == "fifo" and active) or used + need > self.budget:
+                if (one_at_a_time and active) or used + need > self.budget:
                     break
                 a = _Active(pending.pop(0), now)
                 active.append(a)
                 used += a.bytes
-            if not active:
-                if pending:
-                    time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
-                continue
-            sel = self.select(active, mode)
-            chunk = min(self.max_chunk, min(a.remaining for a in sel))
-            by_kind: dict = {}
-            for a in sel:
-                by_kind.setdefault(a.lat.kind, []).append(a)
-            for kind, members in by_kind.items():
-                ids = tuple(id(a) for a in members)
-                cached = batches.get(kind)
-                if cached is None or cached[0] != ids:
-                    if cached is not None:
-                        cached[1].close()
-                    batches[kind] = (ids, Batch([a.lat for a in members]))
-                batches[kind][1].step(chunk)
-            for kind in [k for k in batches if k not in by_kind]:
-                batches.pop(kind)[1].close()
-            torch.cuda.synchronize()
-            rounds += 1
-            finished = []
-            for a in sel:
-                a.remaining -= chunk
-                lups += chunk * a.nodes
-                if a.remaining == 0:
-                    finished.append(a)
-            if finished:
-                drop_batches()
-                t_done = time.perf_counter() - t0
-                for a in finished:
-                    rec = {"rid": a.req.rid, "case": a.req.case, "side": a.req.side, "steps": a.req.steps,
-                           "kind": a.req.kind, "arrival": a.req.arrival, "admitted": a.t_admit,
-                           "completed": t_done, "latency": t_done - a.req.arrival, **a.result()}
-                    if keep_states:
-                        rec["state"] = a.lat.download()
-                    done.append(rec)
-                    active.remove(a)
-                    used -= a.bytes
-                    a.lat.close()
-        drop_batches()
+            t_admit += time.perf_counter() - ta
+
+        try:
+            while pending or active:
+                if not active:
+                    admit(time.perf_counter() - t0)
+                    if not active:
+                        if pending:
+                            time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
+                        continue
+                sel = self.select(active, mode)
+                if mode == "plain":
+                    chunk = sel[0].remaining       # the whole solve, one launch per step
+                    sel[0].lat.step(chunk)
+                else:
+                    chunk = min(self.max_chunk, min(a.remaining for a in sel))
+                    by_kind: dict = {}
+                    for a in sel:
+                        if a.nodes >= self.alone_nodes:
+                            a.lat.step(chunk)
+                        else:
+                            by_kind.setdefault(a.lat.kind, []).append(a)
+                    for kind, members in by_kind.items():
+                        ids = tuple(id(a) for a in members)
+                        cached = batches.get(kind)
+                        if cached is None or cached[0] != ids:
+                            if cached is not None:
+                                cached[1].close()
+                            batches[kind] = (ids, Batch([a.lat for a in members]))
+                        batches[kind][1].step(chunk)
+                    for kind in [k for k in batches if k not in by_kind]:
+                        batches.pop(kind)[1].close()
+                # while the GPU runs the round: admit the requests that arrived
+                if not one_at_a_time:
+                    admit(time.perf_counter() - t0)
+                tw = time.perf_counter()
+                torch.cuda.synchronize()
+                t_wait += time.perf_counter() - tw
+                rounds += 1
+                finished = []
+                for a in sel:
+                    a.remaining -= chunk
+                    lups += chunk * a.nodes
+                    if a.remaining == 0:
+                        finished.append(a)
+                if finished:
+                    gone = {id(a) for a in finished}
+                    for kind in [k for k, (ids, _) in batches.items() if gone & set(ids)]:
+                        batches.pop(kind)[1].close()     # a batch goes before its lattices
+                    t_done = time.perf_counter() - t0
+                    for a in finished:
+                        rec = {"rid": a.req.rid, "case": a.req.case, "side": a.req.side, "steps": a.req.steps,
+                               "kind": a.req.kind, "arrival": a.req.arrival, "admitted": a.t_admit,
+                               "completed": t_done, "latency": t_done - a.req.arrival, **a.result()}
+                        if keep_states:
+                            rec["state"] = a.lat.download()
+                        done.append(rec)
+                        active.remove(a)
+                        used -= a.bytes
+                        a.lat.close()
+            for _, b in batches.values():
+                b.close()
+        finally:
+            set_retained_bytes(0)
         wall = time.perf_counter() - t0
         lat = np.array([d["latency"] for d in done])
         summary = {"mode": mode, "requests": len(done), "wall_s": wall, "rounds": rounds,
                    "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                    "mean_latency_s": float(lat.mean()), "aggregate_glups": lups / wall / 1e9,
-                   "solves_per_s": len(done) / wall, "budget_gb": self.budget / 1e9}
+                   "solves_per_s": len(done) / wall, "budget_gb": self.budget / 1e9,
+                   "host_admission_s": t_admit, "gpu_wait_s": t_wait}
         return done, summary
 
 
@@ -217,8 +257,9 @@ def main(argv=None):
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--budget-gb", type=float, default=150.0)
-    ap.add_argument("--modes", default="continuous,shared,fifo")
+    ap.add_argument("--modes", default="continuous,shared,fifo,plain")
     ap.add_argument("--floor-nodes", type=float, default=8e6)
+    ap.add_argument("--alone-nodes", type=float, default=2e6)
     ap.add_argument("--max-side", type=int, default=256)
     ap.add_argument("--max-steps", type=int, default=10000)
     args = ap.parse_args(argv)
@@ -228,13 +269,16 @@ def main(argv=None):
                      "side": [32, args.max_side], "steps": [500, args.max_steps],
                      "total_lups": sum(r.side ** 3 * (2 if r.case == "sphere" else 1) * r.steps for r in trace)}}
     for mode in args.modes.split(","):
-        _, summary = Server(args.budget_gb * 1e9, floor_nodes=args.floor_nodes).run(trace, mode=mode)
+        _, summary = Server(args.budget_gb * 1e9, floor_nodes=args.floor_nodes, alone_nodes=args.alone_nodes).run(trace, mode=mode)
         out[mode] = summary
         print(json.dumps({mode: summary}), flush=True)
     if "continuous" in out and "fifo" in out:
         out["p50_speedup_vs_fifo"] = out["fifo"]["p50_latency_s"] / out["continuous"]["p50_latency_s"]
         out["p99_speedup_vs_fifo"] = out["fifo"]["p99_latency_s"] / out["continuous"]["p99_latency_s"]
         out["solves_per_s_vs_fifo"] = out["continuous"]["solves_per_s"] / out["fifo"]["solves_per_s"]
+    if "continuous" in out and "plain" in out:
+        out["solves_per_s_vs_plain"] = out["continuous"]["solves_per_s"] / out["plain"]["solves_per_s"]
+        out["p99_speedup_vs_plain"] = out["plain"]["p99_latency_s"] / out["continuous"]["p99_latency_s"]
     print(json.dumps(out), flush=True)
     return 0
 

@@ -47,14 +47,33 @@ void bgk_lattice_desc_init(bgk_lattice_desc* d, int kind, int bcase, int l, int 
 /* Device bytes a lattice with this description occupies (admission control). */
 size_t bgk_lattice_device_bytes(const bgk_lattice_desc* d);
 
-/* Allocate the lattice on the current device (cudaMalloc). */
+/* Allocate the lattice on the current device.  Lattices, batches and their
+   masks and workspaces come from one stream-ordered memory pool per device;
+   creation zeroes the populations on a private stream, so it does not wait
+   for kernels in flight on other streams.  Destruction waits for the device,
+   like cudaFree. */
 int bgk_lattice_create(const bgk_lattice_desc* d, bgk_lattice** out);
 int bgk_lattice_destroy(bgk_lattice* lat);
+
+/* Bytes of freed lattice memory the current device's pool keeps for reuse
+   (default 0: freed memory goes back to the device at once).  A server that
+   creates and destroys many lattices sets its budget here, so that creation
+   reuses memory instead of mapping it anew. */
+int bgk_set_retained_bytes(size_t bytes);
+/* Give every unused block of the current device's pool back to the device. */
+int bgk_trim_memory(void);
 
 /* Obstacle mask obs_host[l*m*n] (i fastest, 1 = solid, SRC/build.obs.F90
    convention); copied to the device, bounding box computed here.  Must stay
    one node inside the lattice.  NULL removes the obstacle. */
 int bgk_lattice_set_obstacle(bgk_lattice* lat, const int32_t* obs_host);
+
+/* Solid sphere obstacle built on the device: nodes with (i - cx)^2 +
+   (j - cy)^2 + (k - cz)^2 <= r2 are solid (the mask bgk_lattice_set_obstacle
+   would get from the same rule on the host; bounding box gathered on the
+   device).  Same validation; synchronous.  No counterpart in the reference
+   (SRC/build.obs.F90 builds a shell on the host). */
+int bgk_lattice_set_sphere(bgk_lattice* lat, double cx, double cy, double cz, double r2);
 
 /* Load / store the post-collision state in the reference layout (see top).
    Stream-ordered; host memory should be pinned for asynchrony.  store needs

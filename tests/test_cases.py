@@ -35,11 +35,17 @@ def test_reference_shell_matches_loop_restatement():
 
 def test_solid_sphere_of_benchmark_config():
     case = CS.sphere()
-    obs = case["obstacle"]
+    obs = CS.obstacle_mask(case)
     assert obs.shape == (256, 256, 512)
     # D = 40 centred at (128,128,128): 4/3 pi 20^3 ~ 33510 nodes
     assert abs(int(obs.sum()) - 4.0 / 3.0 * np.pi * 20 ** 3) < 600
     assert case["drag_box"] == (105, 151, 105, 151, 105, 151)
+    # the analytic bounding box is the mask's
+    assert CS.sphere_bbox(512, 256, 256, 40.0, (128, 128, 128)) == CS._bbox(obs)
+    for l, m, n, dia, c in [(64, 32, 32, 9.0, (20.5, 16.0, 15.3)), (48, 24, 24, 6.0, (12, 12, 12)),
+                            (40, 20, 12, 5.5, (10.2, 9.7, 6.1))]:
+        o, b = CS.solid_sphere_obstacle(l, m, n, dia, c)
+        assert CS.sphere_bbox(l, m, n, dia, c) == b
     assert abs(1.0 / case["omega"] - (3 * 0.05 * 40 / 300 + 0.5)) < 1e-15
 
 
@@ -52,3 +58,15 @@ def test_collision_parameters():
     assert abs(CS.omega_from_nu(0.032) - 1 / 0.596) < 1e-12
     pof = CS.poiseuille(32, 0.6)
     assert pof["force_mode"] == 1 and pof["force"][0] == 1e-7
+
+
+def test_serve_extents_match_cases():
+    """The server sizes a request from its extents alone; they must be the
+    extents of the case it builds."""
+    from bgk3d_gpu_b200 import serve as S
+    for case in ("ldc", "tgv", "sphere"):
+        for side in (8, 34, 96):
+            req = S.Request(0, 0.0, case, side, 10, 0.6, "f32")
+            c = S.case_of(req)
+            assert S.extents(req) == (c["l"], c["m"], c["n"], c["bcase"])
+            assert abs(c["omega"] - 1.0 / req.tau) == 0.0

@@ -94,3 +94,45 @@ def test_aa_odd_step_has_no_observable_state():
         lat.moments()
     lat.step(1)
     lat.download()
+
+
+@pytest.mark.parametrize("pattern", ["ab", "aa"])
+@pytest.mark.parametrize("center,diameter", [((12, 10, 9), 7.0), ((4.5, 5.0, 12.2), 5.0), ((30.0, 2.0, 2.0), 0.5),
+                                             ((0.5, 0.5, 0.5), 0.5)])
+def test_device_sphere_matches_host_mask(pattern, center, diameter):
+    """bgk_lattice_set_sphere builds the same obstacle as the host mask: the
+    solves from both are bit-identical (the mask and its bounding box decide
+    every solid test)."""
+    from bgk3d_gpu_b200 import cases as CS
+    from bgk3d_gpu_b200.lattice import Lattice
+    l, m, n = 32, 20, 18
+    case = CS.sphere(l, m, n, kind="f32", diameter=diameter, center=center)
+    mask = CS.obstacle_mask(case)
+    st = None
+    out = []
+    for dev in (True, False):
+        lat = Lattice(l, m, n, kind=1, bcase="inflow", omega=case["omega"], pattern=pattern, u_inflow=0.05)
+        if dev:
+            lat.set_sphere(*case["sphere"])
+        else:
+            lat.set_obstacle(mask)
+        if st is None:
+            st = random_state(l, m, n, 1, seed=5)
+        lat.upload(st)
+        lat.step(6)
+        out.append(lat.download())
+        lat.close()
+    assert np.array_equal(out[0], out[1])
+
+
+def test_device_sphere_touching_the_walls_is_refused_like_the_mask():
+    from bgk3d_gpu_b200 import cases as CS
+    from bgk3d_gpu_b200._lib import BGKError
+    from bgk3d_gpu_b200.lattice import Lattice
+    case = CS.sphere(32, 20, 18, kind="f32", diameter=9.0, center=(1.5, 2.0, 17.2))
+    lat = Lattice(32, 20, 18, kind=1, bcase="inflow", omega=1.5, u_inflow=0.05)
+    with pytest.raises(BGKError):
+        lat.set_sphere(*case["sphere"])
+    with pytest.raises(BGKError):
+        lat.set_obstacle(CS.obstacle_mask(case))
+    lat.close()

@@ -76,8 +76,11 @@ def test_fifo_mode_and_memory_budget():
     # a budget that fits one or two solves at a time forces queueing
     done, summary = Server(budget_bytes=2.2 * biggest, max_chunk=40).run(trace, keep_states=True)
     done_f, summary_f = Server(budget_bytes=20e9).run(trace, mode="fifo", keep_states=True)
+    done_p, summary_p = Server(budget_bytes=20e9).run(trace, mode="plain", keep_states=True)
     a = {d["rid"]: d["state"] for d in done}
     b = {d["rid"]: d["state"] for d in done_f}
+    c = {d["rid"]: d["state"] for d in done_p}
     for rid in a:
         assert np.array_equal(a[rid], b[rid])
-    assert summary_f["requests"] == summary["requests"] == len(trace)
+        assert np.array_equal(a[rid], c[rid])
+    assert summary_f["requests"] == summary["requests"] == summary_p["requests"] == len(trace)
