@@ -97,6 +97,8 @@ def lib() -> ctypes.CDLL:
     L.bgk_last_error.restype = c_char_p
     L.bgk_version.argtypes = []
     L.bgk_version.restype = c_char_p
+    L.bgk_set_pair_kernels.argtypes = [c_int]
+    L.bgk_set_pair_kernels.restype = c_int
     _bind_lattice(L)
     _lib = L
     return L

@@ -112,6 +112,12 @@ int bgk::draglift_launch(const bgk_sweep_params* p, void* const* a, int is, int 
 
 extern "C" {
 
+int bgk_set_pair_kernels(int enable) {
+    const int prev = g_pair_kernels ? 1 : 0;
+    g_pair_kernels = enable != 0;
+    return prev;
+}
+
 void bgk_sweep_params_init(bgk_sweep_params* p, int kind, int l, int m, int n, double omega) {
     std::memset(p, 0, sizeof *p);
     p->kind = kind; p->bcase = BGK_BC_NONE;

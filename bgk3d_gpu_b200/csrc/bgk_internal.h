@@ -9,6 +9,9 @@ namespace bgk {
 // Off by default: bit-exact, 280 instead of 408 instructions per node for
 // FP16, but measured at half the one-node kernel's rate on 256^3 (B200).
 inline bool g_tma_kernels = false;
+// Two-node sweep for the 16-bit kinds (sweep_ab2_kernel): on by default;
+// bgk_set_pair_kernels(0) selects the one-node sweep (tests compare both).
+inline bool g_pair_kernels = true;
 // Record a formatted message as the calling thread's last error; returns code.
 int set_error(int code, const char* fmt, ...);
 // cudaGetLastError after a launch, recorded as an error when it failed.

@@ -96,6 +96,17 @@ template <> __device__ __forceinline__ __nv_bfloat16 ldro<__nv_bfloat16>(const _
 // Unsigned 32-bit division by a runtime constant with a multiply-high and a
 // shift (Granlund & Montgomery, "Division by invariant integers using
 // multiplication", PLDI 1994, round-up variant).  Exact for every n < 2^32.
+// Resident 256-thread blocks per SM that the two-lattice one-node sweep is
+// compiled for (the register cap follows: 64K / (256 x blocks)).  FP64
+// compute needs the most registers; the 16-bit kinds move half the bytes of
+// FP32 per node, so they need more warps in flight to cover memory latency
+// (5 blocks = 48 registers; measured on 256^3 against 4 blocks: FP16 +5 %
+// periodic, +6 % driven).  The in-place and batched sweeps keep 4: they
+// spill at 48.
+template <class S, class C> struct SweepBlocks {
+    static constexpr int value = sizeof(C) == 8 ? 3 : (sizeof(S) == 2 ? 5 : 4);
+};
+
 struct FastDiv {
     uint32_t d, mul, shift;
     __host__ void init(uint32_t divisor) {

@@ -58,6 +58,12 @@ template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbLaunch
         sweep_ab_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
     }
 };
+template <class S, class C, int BC, class IDX, int CM, bool OBS> struct Ab2Launch {
+    static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
+        if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && !OBS)
+            sweep_ab2_kernel<S, C, BC, IDX, CM><<<blocks, 256, 0, st>>>(A);
+    }
+};
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AaEvenLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
         aa_even_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
@@ -91,6 +97,26 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     const int cm = coll_mode(A);
     const bool obs = A.obs != nullptr;
     const unsigned nb = (unsigned)blocks;
+    if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
+        if (g_pair_kernels && cm_fast(cm) && !obs && mom == nullptr && nelem < (1LL << 31)) {
+            // two nodes per thread: 64-element segments (fused collision only:
+            // with the reference-order collision the kernel spills and is
+            // slower than the one-node sweep)
+            SweepArgs<S, C> A2 = A;
+            A2.nseg = (A.nseg + 1) / 2;
+            A2.div_seg.init((uint32_t)A2.nseg);
+            const long long w2 = (long long)A2.nseg * p->m * p->n;
+            const unsigned nb2 = (unsigned)((w2 + 7) / 8);
+            switch (p->bcase) {
+                case BC_NONE: by_variant<Ab2Launch, S, C, BC_NONE>(nelem, cm, false, A2, nb2, st); break;
+                case BC_DRIVEN: by_variant<Ab2Launch, S, C, BC_DRIVEN>(nelem, cm, false, A2, nb2, st); break;
+                case BC_PERIODIC: by_variant<Ab2Launch, S, C, BC_PERIODIC>(nelem, cm, false, A2, nb2, st); break;
+                case BC_CHANNEL: by_variant<Ab2Launch, S, C, BC_CHANNEL>(nelem, cm, false, A2, nb2, st); break;
+                case BC_INFLOW: by_variant<Ab2Launch, S, C, BC_INFLOW>(nelem, cm, false, A2, nb2, st); break;
+            }
+            return check_launch("sweep_ab2_kernel");
+        }
+    }
     switch (p->bcase) {
         case BC_NONE: by_variant<AbLaunch, S, C, BC_NONE>(nelem, cm, obs, A, nb, st); break;
         case BC_DRIVEN: by_variant<AbLaunch, S, C, BC_DRIVEN>(nelem, cm, obs, A, nb, st); break;

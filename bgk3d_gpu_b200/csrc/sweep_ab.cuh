@@ -30,6 +30,7 @@
 // copies would otherwise read solid-node garbage.
 #pragma once
 #include "d3q19.cuh"
+#include "f2.cuh"
 #include "reduce.cuh"
 
 namespace bgk {
@@ -254,10 +255,60 @@ __device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j,
 // FP64 sums of SRC/diagno.F90's per-node moments of the state it produced
 // (fluid nodes) to P.mom[blockIdx.x * 5 ..].
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
-__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) sweep_ab_kernel(const SweepArgs<S, C> P) {
+__global__ void __launch_bounds__(256, (SweepBlocks<S, C>::value)) sweep_ab_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     sweep_node<S, C, BC, IDX, CM, OBS>(P, blockIdx.x * 8u + (threadIdx.x >> 5), m5);
     if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
+}
+
+// Two nodes per thread for the 16-bit kinds: a warp owns 64 consecutive
+// elements of one row (two 32-element segments, P.nseg counting 64-element
+// segments), lane t the nodes at t and t + 32.  Each node is gathered by the
+// one-node rules (gather_at); the two collisions run as one on packed FP32
+// pairs (FADD2 / FFMA2, lane-wise the same roundings, so the result is
+// bit-identical to the one-node sweep) and the stores stay 16-bit and
+// coalesced.  Per node this halves the collision's instructions and shares
+// the row/segment arithmetic.  No obstacle and no fused moments (the host
+// takes the one-node kernel for those).
+template <class S, class C, int BC, class IDX, int CM>
+__global__ void __launch_bounds__(256, 4) sweep_ab2_kernel(const SweepArgs<S, C> P) {
+    static_assert(sizeof(S) == 2 && sizeof(C) == 4, "two-node sweep: 16-bit storage, float compute");
+    const uint32_t gw = blockIdx.x * 8u + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const uint32_t row = P.div_seg.div(gw);
+    if (row >= P.nrows) return;
+    const int seg = (int)(gw - row * (uint32_t)P.nseg);
+    const uint32_t kk = P.div_m.div(row);
+    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
+    const int k = (int)kk + 1;
+    const IDX nx = (IDX)P.nx, nxy = (IDX)P.nxy;
+    const IDX rowoff = nx * (IDX)j + nxy * (IDX)k;
+    const int sh = (int)((P.align_base + (long long)rowoff + 1) & 31);
+    int ia = seg * 64 + lane + 1 - (P.nseg_aligned ? 0 : sh);
+    int ib = ia + 32;
+    const bool va = ia >= 1 && ia <= P.l, vb = ib >= 1 && ib <= P.l;
+    if (!va && !vb) return;
+    if (!va) ia = ib;          // compute the valid node twice, store it once
+    if (!vb) ib = ia;
+    C xa[19], xb[19];
+    gather_at<S, C, BC, IDX, false>(P, ia, j, k, xa);
+    gather_at<S, C, BC, IDX, false>(P, ib, j, k, xb);
+    F2 x[19], y[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) x[d] = F2(xa[d], xb[d]);
+    if constexpr (cm_fast(CM))
+        bgk_collide_fast_v<F2, float, cm_generic(CM), Scaled<S>::value>(x, y, P.fc, P.inv_scale);
+    else
+        bgk_collide_v<F2, float, cm_generic(CM), Scaled<S>::value>(x, y, P.col, P.inv_scale);
+    typedef Pack2<S> PK;
+    const IDX ca = rowoff + (IDX)ia, cb = rowoff + (IDX)ib;
+#pragma unroll
+    for (int d = 0; d < 19; ++d) {
+        const typename PK::V w = PK::pack(y[d]);
+        S* dst = d < 18 ? P.b[d] : const_cast<S*>(P.a[18]);
+        if (va) dst[ca] = PK::lo(w);
+        if (vb) dst[cb] = PK::hi(w);
+    }
 }
 
 // Outflow halo plane for the inflow case: a10..a14(l+1, j, k) from the

@@ -77,7 +77,8 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--modes", default="strict", help="collision modes: strict, fast or both (strict,fast)")
-    ap.add_argument("--tma", default="on", help="TMA-staged AB sweep: on, off or both (on,off)")
+    ap.add_argument("--tma", default="off", help="TMA-staged AB sweep: on, off or both (on,off)")
+    ap.add_argument("--pair", default="on", help="two-node sweep of the 16-bit kinds: on, off or both (on,off)")
     args = ap.parse_args(argv)
     from ._lib import lib
     l, m, n = args.size
@@ -89,22 +90,32 @@ def main(argv=None) -> int:
                     if mode == "fast" and kind in ("f64", "f32f64"):
                         continue        # fused collision: float compute only
                     for tma in args.tma.split(","):
-                        if tma == "off" and pattern == "aa":
+                        if tma == "on" and pattern == "aa":
                             continue    # the TMA sweep serves AB lattices
-                        prev = lib().bgk_set_tma_kernels(1 if tma == "on" else 0)
-                        lat = make(kind, pattern, case, l, m, n, fast=(mode == "fast"))
-                        path = "tma" if lat.L.bgk_lattice_uses_tma(lat.h) else "one-node"
-                        s = time_steps(lat, args.steps, args.warmup)
-                        status = lat.L.bgk_lattice_status(lat.h)
-                        lat.close()
-                        lib().bgk_set_tma_kernels(prev)
-                        glups = l * m * n / s / 1e9
-                        gbs = glups * 2 * 19 * BYTES[kind]
-                        print(json.dumps({"kind": kind, "mode": mode, "tma": tma, "path": path, "status": status,
-                                          "pattern": pattern, "case": case, "size": [l, m, n],
-                                          "steps": args.steps, "ms_per_step": s * 1e3, "glups": glups,
-                                          "hbm_gbs": gbs, "frac_of_measured": gbs / peak if peak else None}),
-                              flush=True)
+                        for pair in args.pair.split(","):
+                            if pair == "off" and (BYTES[kind] != 2 or pattern == "aa" or tma == "on"):
+                                continue    # the two-node sweep serves 16-bit AB lattices
+                            prev = lib().bgk_set_tma_kernels(1 if tma == "on" else 0)
+                            prev_pair = lib().bgk_set_pair_kernels(1 if pair == "on" else 0)
+                            lat = make(kind, pattern, case, l, m, n, fast=(mode == "fast"))
+                            if lat.L.bgk_lattice_uses_tma(lat.h):
+                                path = "tma"
+                            elif pair == "on" and BYTES[kind] == 2 and pattern == "ab" and case != "inflow":
+                                path = "two-node"
+                            else:
+                                path = "one-node"
+                            s = time_steps(lat, args.steps, args.warmup)
+                            status = lat.L.bgk_lattice_status(lat.h)
+                            lat.close()
+                            lib().bgk_set_tma_kernels(prev)
+                            lib().bgk_set_pair_kernels(prev_pair)
+                            glups = l * m * n / s / 1e9
+                            gbs = glups * 2 * 19 * BYTES[kind]
+                            print(json.dumps({"kind": kind, "mode": mode, "tma": tma, "path": path,
+                                              "status": status, "pattern": pattern, "case": case,
+                                              "size": [l, m, n], "steps": args.steps, "ms_per_step": s * 1e3,
+                                              "glups": glups, "hbm_gbs": gbs,
+                                              "frac_of_measured": gbs / peak if peak else None}), flush=True)
     return 0
 
 

@@ -1,0 +1,85 @@
+"""The two-node sweep of the 16-bit kinds (sweep_ab2_kernel: nodes i and
+i + 32 per thread, packed FP32 collision; taken with the fused-multiply-add
+collision) against the one-node sweep: bit-identical states for FP16 and
+BF16 storage, every boundary case, force-free and forced collisions, on
+library-owned lattices (aligned rows) and on the reference layout with odd
+paddings (rows starting anywhere in a segment), with row lengths that leave
+partial 64-node segments."""
+import zlib
+
+import numpy as np
+import pytest
+
+from _cases import BCASE, CASE_PARAMS, OMEGA, SCALE, interior, random_state
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["driven", "periodic", "channel", "channel_const", "inflow", "none"]
+SHAPES = [(70, 13, 9), (128, 12, 6), (33, 22, 5), (200, 5, 4)]
+
+
+def _switch(on: bool) -> int:
+    from bgk3d_gpu_b200._lib import lib
+    return lib().bgk_set_pair_kernels(1 if on else 0)
+
+
+def _lattice(kind, case, shape, fast, on, steps=5):
+    from bgk3d_gpu_b200.lattice import Lattice
+    l, m, n = shape
+    p = CASE_PARAMS[case]
+    prev = _switch(on)
+    try:
+        lat = Lattice(l, m, n, kind=kind, bcase=BCASE[case], omega=OMEGA, scale=SCALE[kind], fast=fast,
+                      lid_force=p.get("lid_force", 0.0), u_inflow=p.get("u_inflow", 0.0),
+                      force_mode=p.get("force_mode", 0), force=p.get("force", (0.0, 0.0, 0.0)))
+        seed = zlib.crc32(repr((kind, case, shape)).encode()) % 1000
+        lat.upload(random_state(l, m, n, kind, seed=seed, scale=SCALE[kind]))
+        lat.step(steps)
+        out = interior(lat.download(), l, m, n)
+        lat.close()
+    finally:
+        _switch(bool(prev))
+    return out
+
+
+def _reference_layout(kind, case, shape, fast, on, ipad, jpad, steps=3):
+    from bgk3d_gpu_b200.lattice import DeviceLattice
+    l, m, n = shape
+    prev = _switch(on)
+    try:
+        dev = DeviceLattice(l, m, n, kind=kind, bcase=BCASE[case], omega=OMEGA, ipad=ipad, jpad=jpad,
+                            scale=SCALE[kind], fast=fast, **CASE_PARAMS[case])
+        seed = zlib.crc32(repr((kind, case, shape, ipad)).encode()) % 1000
+        dev.upload(random_state(l, m, n, kind, seed=seed, ipad=ipad, jpad=jpad, scale=SCALE[kind]))
+        dev.step(steps)
+        out = dev.download()[:, 1:n + 1, 1:m + 1, 1:l + 1]
+    finally:
+        _switch(bool(prev))
+    return out
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+@pytest.mark.parametrize("case", [c for c in CASES if c != "none"])
+def test_pair_equals_one_node_sweep_on_lattices(kind, case):
+    for shape in SHAPES:
+        a = _lattice(kind, case, shape, True, True)
+        b = _lattice(kind, case, shape, True, False)
+        bad = np.argwhere(a != b)
+        assert len(bad) == 0, (kind, case, shape, len(bad), bad[:5].tolist())
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("ipad,jpad", [(0, 0), (5, 1), (13, 0)])
+def test_pair_equals_one_node_sweep_on_reference_layout(kind, case, ipad, jpad):
+    for shape in SHAPES[:3]:
+        a = _reference_layout(kind, case, shape, True, True, ipad, jpad)
+        b = _reference_layout(kind, case, shape, True, False, ipad, jpad)
+        bad = np.argwhere(a != b)
+        assert len(bad) == 0, (kind, case, shape, ipad, len(bad), bad[:5].tolist())
+
+
+def test_pair_switch_default_on():
+    prev = _switch(True)
+    assert _switch(bool(prev)) == 1
+    assert prev == 1
