@@ -61,4 +61,20 @@ template <> struct Pack2<__nv_bfloat16> {
     static __device__ __forceinline__ __nv_bfloat16 hi(V w) { return __high2bfloat16(w); }
 };
 
+// Bits of a 16-bit storage value, and two packed values <-> one 32-bit word
+// (lo = first element in memory).
+__device__ __forceinline__ uint32_t s_bits(__half v) { return __half_as_ushort(v); }
+__device__ __forceinline__ uint32_t s_bits(__nv_bfloat16 v) { return __bfloat16_as_ushort(v); }
+template <class S> __device__ __forceinline__ F2 raw_bits(uint32_t w) {
+    typename Pack2<S>::V v;
+    memcpy(&v, &w, sizeof w);
+    return Pack2<S>::raw(v);
+}
+template <class S> __device__ __forceinline__ uint32_t pack_bits(F2 a) {
+    const typename Pack2<S>::V v = Pack2<S>::pack(a);
+    uint32_t w;
+    memcpy(&w, &v, sizeof w);
+    return w;
+}
+
 }  // namespace bgk

@@ -64,6 +64,24 @@ template <class S, class C, int BC, class IDX, int CM, bool OBS> struct Ab2Launc
             sweep_ab2_kernel<S, C, BC, IDX, CM><<<blocks, 256, 0, st>>>(A);
     }
 };
+template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbpLaunch {
+    static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
+        if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && !OBS && sizeof(IDX) == 4)
+            sweep_abp_kernel<S, C, BC, CM><<<blocks, kPairThreads, 0, st>>>(A);
+    }
+};
+// True when every node pair (i, i + 1), i odd, is one aligned 32-bit word in
+// every population plane of a and b: even row pitches and each plane's base
+// at 2 mod 4 bytes (then element 1 of every row starts a word).
+template <class S>
+bool pairs_aligned(const bgk_sweep_params* p, void* const* a, void* const* b) {
+    if (sizeof(S) != 2 || (p->l & 1) || (p->nx & 1) || ((p->nx * p->ny) & 1)) return false;
+    for (int d = 0; d < 19; ++d)
+        if (((uintptr_t)a[d] & 3u) != 2u) return false;
+    for (int d = 0; d < 18; ++d)
+        if (((uintptr_t)b[d] & 3u) != 2u) return false;
+    return true;
+}
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AaEvenLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
         aa_even_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
@@ -98,6 +116,24 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     const bool obs = A.obs != nullptr;
     const unsigned nb = (unsigned)blocks;
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
+        if (g_pair_kernels && cm_fast(cm) && !obs && mom == nullptr && nelem < (1LL << 31) &&
+            pairs_aligned<S>(p, a, b)) {
+            // adjacent node pairs: 64-node segments from i = 1
+            SweepArgs<S, C> A2 = A;
+            A2.nseg = (p->l + 63) / 64;
+            A2.div_seg.init((uint32_t)A2.nseg);
+            const long long w2 = (long long)A2.nseg * p->m * p->n;
+            constexpr int wpb = kPairThreads / 32;
+            const unsigned nb2 = (unsigned)((w2 + wpb - 1) / wpb);
+            switch (p->bcase) {
+                case BC_NONE: by_variant<AbpLaunch, S, C, BC_NONE>(nelem, cm, false, A2, nb2, st); break;
+                case BC_DRIVEN: by_variant<AbpLaunch, S, C, BC_DRIVEN>(nelem, cm, false, A2, nb2, st); break;
+                case BC_PERIODIC: by_variant<AbpLaunch, S, C, BC_PERIODIC>(nelem, cm, false, A2, nb2, st); break;
+                case BC_CHANNEL: by_variant<AbpLaunch, S, C, BC_CHANNEL>(nelem, cm, false, A2, nb2, st); break;
+                case BC_INFLOW: by_variant<AbpLaunch, S, C, BC_INFLOW>(nelem, cm, false, A2, nb2, st); break;
+            }
+            return check_launch("sweep_abp_kernel");
+        }
         if (g_pair_kernels && cm_fast(cm) && !obs && mom == nullptr && nelem < (1LL << 31)) {
             // two nodes per thread: 64-element segments (fused collision only:
             // with the reference-order collision the kernel spills and is

@@ -311,6 +311,113 @@ __global__ void __launch_bounds__(256, 4) sweep_ab2_kernel(const SweepArgs<S, C>
     }
 }
 
+// Adjacent node pairs for the 16-bit kinds on aligned rows of even length:
+// a warp owns 64 consecutive nodes of one row, lane t the pair (i, i + 1)
+// with i = 64 seg + 2t + 1 (i odd, so the pair is one aligned 32-bit word in
+// every plane).  Per population one 32-bit load fetches the pair at the
+// source row (y/z offsets and their wraps are the same for the whole warp):
+//   c_x =  0: both values;
+//   c_x = +1: node i + 1 takes the low half, node i the high half of lane
+//             t - 1's word (a shuffle);
+//   c_x = -1: node i takes the high half, node i + 1 the low half of lane
+//             t + 1's word.
+// The value the warp does not hold (lane 0's left, lane 31's right
+// neighbour) and the x faces (i = 1, i + 1 = l) are resolved per node by the
+// one-node rules (gather_at): wrap, bounce-back, inflow equilibrium, outflow
+// halo.  A y/z wall bounces both nodes to their own opposite populations
+// (one aligned load).  The two collisions run as one on packed FP32 pairs
+// (bit-identical to the one-node sweep) and every store is one aligned
+// 32-bit word.  No obstacle, no fused moments, 32-bit element offsets.
+constexpr int kPairThreads = 128;   // threads per block of sweep_abp_kernel
+constexpr int kPairBlocks = 7;      // resident blocks per SM it is compiled for (72 registers)
+template <class S, class C, int BC, int CM>
+__global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(const SweepArgs<S, C> P) {
+    static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair sweep: 16-bit storage, float compute");
+    typedef Faces<BC> F;
+    const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const uint32_t row = P.div_seg.div(gw);
+    if (row >= P.nrows) return;                       // whole warp
+    const int seg = (int)(gw - row * (uint32_t)P.nseg);
+    const uint32_t kk = P.div_m.div(row);
+    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
+    const int k = (int)kk + 1;
+    const int nx = (int)P.nx, nxy = (int)P.nxy;
+    const int i0 = seg * 64 + 2 * lane + 1;
+    const bool valid = i0 < P.l;                      // l even: the pair (i0, i0 + 1) is inside
+    const int ia = valid ? i0 : P.l - 1;              // other lanes read a valid pair, store nothing
+    const int c = nx * j + nxy * k + ia;
+    const bool at_lo = ia == 1, at_hi = ia + 1 == P.l;
+    const bool edge_lo = lane == 0 || at_lo, edge_hi = lane == 31 || at_hi;
+    const int oym = (F::PY && j == 1) ? (P.m - 1) * nx : -nx;
+    const int oyp = (F::PY && j == P.m) ? (1 - P.m) * nx : nx;
+    const int ozm = (F::PZ && k == 1) ? (P.n - 1) * nxy : -nxy;
+    const int ozp = (F::PZ && k == P.n) ? (1 - P.n) * nxy : nxy;
+    const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
+    const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
+    // all loads first (no branch between them, so they are in flight
+    // together): the pair word of every population and, for c_x != 0, the
+    // one element the lane may need from outside its warp or across a face
+    uint32_t w[18], e[18];
+    bool wall[18];
+#pragma unroll
+    for (int d = 0; d < 18; ++d) {
+        const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+        bool wl = false;
+        int off = c;
+        if (cy == 1) { off += oym; wl |= wym; } else if (cy == -1) { off += oyp; wl |= wyp; }
+        if (cz == 1) { off += ozm; wl |= wzm; } else if (cz == -1) { off += ozp; wl |= wzp; }
+        wall[d] = wl;
+        // a y/z wall (same for the whole warp): both nodes bounce back
+        const S* src = wl ? P.a[opp_of(d)] + c : P.a[d] + off;
+        w[d] = __ldg(reinterpret_cast<const unsigned*>(src));
+        if (cx == 1) {
+            const S* ep = (F::WX && at_lo) ? P.a[opp_of(d)] + c
+                                           : P.a[d] + off + ((F::PX && at_lo) ? P.l - 1 : -1);
+            e[d] = s_bits(ldro<S>(ep));
+        } else if (cx == -1) {
+            const S* ep = (F::WX && at_hi) ? P.a[opp_of(d)] + c + 1
+                                           : P.a[d] + off + ((F::PX && at_hi) ? 2 - P.l : 2);
+            e[d] = s_bits(ldro<S>(ep));
+        }
+    }
+    F2 x[19];
+#pragma unroll
+    for (int d = 0; d < 18; ++d) {
+        const int cx = cx_of(d);
+        uint32_t v = w[d];
+        if (cx == 1) {
+            // node i + 1: low half; node i: lane t - 1's high half, or the edge value
+            const uint32_t left = __shfl_up_sync(0xffffffffu, v, 1) >> 16;
+            uint32_t lo = edge_lo ? e[d] : left;
+            if (BC == BC_INFLOW && at_lo)
+                lo = s_bits(Conv<S, C>::pack(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col)));
+            if (!wall[d]) v = __byte_perm(lo, v, 0x5410);
+        } else if (cx == -1) {
+            // node i: high half; node i + 1: lane t + 1's low half, or the edge value
+            const uint32_t right = __shfl_down_sync(0xffffffffu, v, 1) & 0xffffu;
+            const uint32_t hi = edge_hi ? e[d] : right;
+            if (!wall[d]) v = __byte_perm(v, hi, 0x5432);
+        }
+        F2 f = raw_bits<S>(v);
+        if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n) {
+            f.v.x = roundtrip<S, C>(d == 1 ? f.v.x + P.lid_force : f.v.x - P.lid_force);
+            f.v.y = roundtrip<S, C>(d == 1 ? f.v.y + P.lid_force : f.v.y - P.lid_force);
+        }
+        x[d] = f;
+    }
+    x[18] = raw_bits<S>(*reinterpret_cast<const unsigned*>(P.a[18] + c));
+    F2 y[19];
+    if constexpr (cm_fast(CM))
+        bgk_collide_fast_v<F2, float, cm_generic(CM), Scaled<S>::value>(x, y, P.fc, P.inv_scale);
+    else
+        bgk_collide_v<F2, float, cm_generic(CM), Scaled<S>::value>(x, y, P.col, P.inv_scale);
+    if (!valid) return;
+#pragma unroll
+    for (int d = 0; d < 18; ++d) *reinterpret_cast<unsigned*>(P.b[d] + c) = pack_bits<S>(y[d]);
+    *reinterpret_cast<unsigned*>(const_cast<S*>(P.a[18]) + c) = pack_bits<S>(y[18]);
+}
+
 // Outflow halo plane for the inflow case: a10..a14(l+1, j, k) from the
 // moments of node (l, j, k) at rho = 1 (SRC/bcond.inflow.F90:135-162), over
 // j = 1..m, k = 1..n (the sweep reads the y/z-wrapped position, which is

@@ -100,7 +100,7 @@ def main(argv=None) -> int:
                             lat = make(kind, pattern, case, l, m, n, fast=(mode == "fast"))
                             if lat.L.bgk_lattice_uses_tma(lat.h):
                                 path = "tma"
-                            elif pair == "on" and BYTES[kind] == 2 and pattern == "ab" and case != "inflow":
+                            elif pair == "on" and BYTES[kind] == 2 and pattern == "ab" and case != "inflow" and mode == "fast":
                                 path = "two-node"
                             else:
                                 path = "one-node"
