@@ -279,16 +279,20 @@ __device__ __forceinline__ double rcp_c(double a) { return 1.0 / a; }
 // which is odd in c).  About 140 operations per node instead of 240; not
 // bit-identical to the reference order (the results differ by a few units in
 // the last place of the compute type per step).
-template <class V, class C, bool GENERIC, bool SCALED>
-__device__ __forceinline__ void bgk_collide_fast_v(const V (&x)[19], V (&y)[19], const FastConst<C>& K,
-                                                   float inv) {
-    const V sum = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] + x[11] +
-                  x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18];
+//
+// bgk_collide_fast_f reads population d through xs(d) for the moment sums and
+// through xp(d) for the relaxation, and hands y_d to ys(d, y_d): a caller
+// short of registers can keep the inputs packed and convert them twice, and
+// store each result as soon as it is known.
+template <class V, class C, bool GENERIC, bool SCALED, class XS, class XP, class YS>
+__device__ __forceinline__ void bgk_collide_fast_f(XS xs, XP xp, YS ys, const FastConst<C>& K, float inv) {
+    const V sum = xs(0) + xs(1) + xs(2) + xs(3) + xs(4) + xs(5) + xs(6) + xs(7) + xs(8) + xs(9) + xs(10) +
+                  xs(11) + xs(12) + xs(13) + xs(14) + xs(15) + xs(16) + xs(17) + xs(18);
     const V rho = SCALED ? fma_c(sum, V((C)inv), V(K.cte1)) : sum + V(K.cte1);
     const V ri = rcp_c(rho);
-    const V mx = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
-    const V my = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
-    const V mz = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
+    const V mx = xs(0) + xs(1) + xs(2) + xs(3) + xs(4) - xs(9) - xs(10) - xs(11) - xs(12) - xs(13);
+    const V my = xs(2) + xs(6) + xs(7) + xs(8) + xs(11) - xs(0) - xs(9) - xs(15) - xs(16) - xs(17);
+    const V mz = xs(3) + xs(5) + xs(6) + xs(12) + xs(17) - xs(1) - xs(8) - xs(10) - xs(14) - xs(15);
     const V g = SCALED ? V((C)inv) * ri : ri;
     const V vx = mx * g, vy = my * g, vz = mz * g;
     const V vsq = fma_c(vz, vz, fma_c(vy, vy, vx * vx));
@@ -305,8 +309,8 @@ __device__ __forceinline__ void bgk_collide_fast_v(const V (&x)[19], V (&y)[19],
     auto pair = [&](int dp, int dm, V v, V A, V B, V R, V f) {
         const V sym = fma_c(A, v * v, B);
         const V an = GENERIC ? fma_c(R, v, f) : R * v;
-        y[dp] = fma_c(x[dp], om, sym) + an;
-        y[dm] = fma_c(x[dm], om, sym) - an;
+        ys(dp, fma_c(xp(dp), om, sym) + an);
+        ys(dm, fma_c(xp(dm), om, sym) - an);
     };
     pair(0, 11, vx - vy, A2, B2, R2, fx - fy);
     pair(1, 12, vx - vz, A2, B2, R2, fx - fz);
@@ -317,7 +321,14 @@ __device__ __forceinline__ void bgk_collide_fast_v(const V (&x)[19], V (&y)[19],
     pair(6, 15, vy + vz, A2, B2, R2, fy + fz);
     pair(7, 16, vy, A1, B1, R1, fy);
     pair(8, 17, vy - vz, A2, B2, R2, fy - fz);
-    y[18] = fma_c(x[18], om, B0);
+    ys(18, fma_c(xp(18), om, B0));
+}
+
+template <class V, class C, bool GENERIC, bool SCALED>
+__device__ __forceinline__ void bgk_collide_fast_v(const V (&x)[19], V (&y)[19], const FastConst<C>& K,
+                                                   float inv) {
+    auto xr = [&](int d) { return x[d]; };
+    bgk_collide_fast_f<V, C, GENERIC, SCALED>(xr, xr, [&](int d, V v) { y[d] = v; }, K, inv);
 }
 
 template <class C, bool GENERIC, bool SCALED>

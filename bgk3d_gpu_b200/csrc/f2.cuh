@@ -70,6 +70,22 @@ template <class S> __device__ __forceinline__ F2 raw_bits(uint32_t w) {
     memcpy(&v, &w, sizeof w);
     return Pack2<S>::raw(v);
 }
+// The same conversion, written so that the compiler neither merges it with
+// another conversion of the same word nor keeps the result alive instead of
+// the word (a caller short of registers converts a packed word twice).  Both
+// conversions are exact, so the values equal raw_bits's.
+template <class S> __device__ __forceinline__ F2 raw_bits_again(uint32_t w);
+template <> __device__ __forceinline__ F2 raw_bits_again<__half>(uint32_t w) {
+    float a, b;
+    asm volatile("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\tcvt.f32.f16 %0, lo;\n\tcvt.f32.f16 %1, hi;\n\t}"
+                 : "=f"(a), "=f"(b) : "r"(w));
+    return F2(a, b);
+}
+template <> __device__ __forceinline__ F2 raw_bits_again<__nv_bfloat16>(uint32_t w) {
+    uint32_t a, b;
+    asm volatile("{\n\tshl.b32 %0, %2, 16;\n\tand.b32 %1, %2, 0xffff0000;\n\t}" : "=r"(a), "=r"(b) : "r"(w));
+    return F2(__uint_as_float(a), __uint_as_float(b));
+}
 template <class S> __device__ __forceinline__ uint32_t pack_bits(F2 a) {
     const typename Pack2<S>::V v = Pack2<S>::pack(a);
     uint32_t w;

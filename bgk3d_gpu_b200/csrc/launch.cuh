@@ -66,7 +66,7 @@ template <class S, class C, int BC, class IDX, int CM, bool OBS> struct Ab2Launc
 };
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbpLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
-        if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && !OBS && sizeof(IDX) == 4)
+        if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && !OBS && sizeof(IDX) == 4 && cm_fast(CM))
             sweep_abp_kernel<S, C, BC, CM><<<blocks, kPairThreads, 0, st>>>(A);
     }
 };

@@ -330,22 +330,14 @@ __global__ void __launch_bounds__(256, 4) sweep_ab2_kernel(const SweepArgs<S, C>
 // 32-bit word.  No obstacle, no fused moments, 32-bit element offsets.
 constexpr int kPairThreads = 128;   // threads per block of sweep_abp_kernel
 constexpr int kPairBlocks = 7;      // resident blocks per SM it is compiled for (72 registers)
-template <class S, class C, int BC, int CM>
-__global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(const SweepArgs<S, C> P) {
-    static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair sweep: 16-bit storage, float compute");
+
+// The pairs of one warp in row (j, k): lane's pair starts at node ia; WALLS:
+// the row lies on a y or z wall of the case (compiled separately, so that
+// the rows inside carry no wall logic).
+template <class S, class C, int BC, int CM, bool WALLS>
+__device__ __forceinline__ void abp_row(const SweepArgs<S, C>& P, int j, int k, int lane, int ia, bool valid) {
     typedef Faces<BC> F;
-    const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    const uint32_t row = P.div_seg.div(gw);
-    if (row >= P.nrows) return;                       // whole warp
-    const int seg = (int)(gw - row * (uint32_t)P.nseg);
-    const uint32_t kk = P.div_m.div(row);
-    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
-    const int k = (int)kk + 1;
     const int nx = (int)P.nx, nxy = (int)P.nxy;
-    const int i0 = seg * 64 + 2 * lane + 1;
-    const bool valid = i0 < P.l;                      // l even: the pair (i0, i0 + 1) is inside
-    const int ia = valid ? i0 : P.l - 1;              // other lanes read a valid pair, store nothing
     const int c = nx * j + nxy * k + ia;
     const bool at_lo = ia == 1, at_hi = ia + 1 == P.l;
     const bool edge_lo = lane == 0 || at_lo, edge_hi = lane == 31 || at_hi;
@@ -353,8 +345,8 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(co
     const int oyp = (F::PY && j == P.m) ? (1 - P.m) * nx : nx;
     const int ozm = (F::PZ && k == 1) ? (P.n - 1) * nxy : -nxy;
     const int ozp = (F::PZ && k == P.n) ? (1 - P.n) * nxy : nxy;
-    const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
-    const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
+    const bool wym = WALLS && F::WY && j == 1, wyp = WALLS && F::WY && j == P.m;
+    const bool wzm = WALLS && F::WZ && k == 1, wzp = WALLS && F::WZ && k == P.n;
     // all loads first (no branch between them, so they are in flight
     // together): the pair word of every population and, for c_x != 0, the
     // one element the lane may need from outside its warp or across a face
@@ -381,7 +373,8 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(co
             e[d] = s_bits(ldro<S>(ep));
         }
     }
-    F2 x[19];
+    // the final pair word of every population (storage representation)
+    uint32_t wv[19];
 #pragma unroll
     for (int d = 0; d < 18; ++d) {
         const int cx = cx_of(d);
@@ -399,23 +392,49 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(co
             const uint32_t hi = edge_hi ? e[d] : right;
             if (!wall[d]) v = __byte_perm(v, hi, 0x5432);
         }
-        F2 f = raw_bits<S>(v);
-        if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n) {
+        if (WALLS && BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n) {
+            // lid term, rounded to storage: the packed word holds it exactly
+            F2 f = raw_bits<S>(v);
             f.v.x = roundtrip<S, C>(d == 1 ? f.v.x + P.lid_force : f.v.x - P.lid_force);
             f.v.y = roundtrip<S, C>(d == 1 ? f.v.y + P.lid_force : f.v.y - P.lid_force);
+            v = pack_bits<S>(f);
         }
-        x[d] = f;
+        wv[d] = v;
     }
-    x[18] = raw_bits<S>(*reinterpret_cast<const unsigned*>(P.a[18] + c));
-    F2 y[19];
-    if constexpr (cm_fast(CM))
-        bgk_collide_fast_v<F2, float, cm_generic(CM), Scaled<S>::value>(x, y, P.fc, P.inv_scale);
-    else
-        bgk_collide_v<F2, float, cm_generic(CM), Scaled<S>::value>(x, y, P.col, P.inv_scale);
-    if (!valid) return;
-#pragma unroll
-    for (int d = 0; d < 18; ++d) *reinterpret_cast<unsigned*>(P.b[d] + c) = pack_bits<S>(y[d]);
-    *reinterpret_cast<unsigned*>(const_cast<S*>(P.a[18]) + c) = pack_bits<S>(y[18]);
+    wv[18] = *reinterpret_cast<const unsigned*>(P.a[18] + c);
+    // collision on packed FP32 pairs; the words stay packed (converted for
+    // the moments and again for the relaxation) and each result is stored
+    // as soon as it is known
+    auto xs = [&](int d) { return raw_bits<S>(wv[d]); };
+    auto xp = [&](int d) { return raw_bits_again<S>(wv[d]); };
+    auto ys = [&](int d, F2 y) {
+        if (valid) *reinterpret_cast<unsigned*>((d < 18 ? P.b[d] : const_cast<S*>(P.a[18])) + c) = pack_bits<S>(y);
+    };
+    bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
+}
+
+template <class S, class C, int BC, int CM>
+__global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(const SweepArgs<S, C> P) {
+    static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair sweep: 16-bit storage, float compute");
+    static_assert(cm_fast(CM), "the pair sweep takes the fused collision");
+    typedef Faces<BC> F;
+    const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const uint32_t row = P.div_seg.div(gw);
+    if (row >= P.nrows) return;                       // whole warp
+    const int seg = (int)(gw - row * (uint32_t)P.nseg);
+    const uint32_t kk = P.div_m.div(row);
+    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
+    const int k = (int)kk + 1;
+    const int i0 = seg * 64 + 2 * lane + 1;
+    const bool valid = i0 < P.l;                      // l even: the pair (i0, i0 + 1) is inside
+    const int ia = valid ? i0 : P.l - 1;              // other lanes read a valid pair, store nothing
+    // the driven cavity's rows inside its walls run without wall logic
+    // (measured +12 % at 256^3); for the channel the split costs registers
+    // (spills) and runs slower, so every channel row takes the wall path
+    const bool wall_row = (F::WY && (j == 1 || j == P.m)) || (F::WZ && (k == 1 || k == P.n));
+    if (BC != BC_DRIVEN || wall_row) abp_row<S, C, BC, CM, true>(P, j, k, lane, ia, valid);
+    else abp_row<S, C, BC, CM, false>(P, j, k, lane, ia, valid);
 }
 
 // Outflow halo plane for the inflow case: a10..a14(l+1, j, k) from the
