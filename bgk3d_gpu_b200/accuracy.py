@@ -11,7 +11,7 @@ of steps from the same initial state and the script reports
   * drag / lift        relative error of the momentum-exchange force
                        (SRC/draglift.F90) at the sampled times (obstacle cases).
 
-  python -m bgk3d_gpu_b200.accuracy --case tgv --steps 2000 --every 10
+  python -m bgk3d_gpu_b200.accuracy --case tgv --steps 2000 --every 10 [--modes strict,fast]
   python -m bgk3d_gpu_b200.accuracy --case sphere --steps 20000 --every 100
 """
 from __future__ import annotations
@@ -64,11 +64,11 @@ def velocity_field(lat, scale: float = 1.0):
     return rho, [mm / rho for mm in mom]
 
 
-def run_case(case: dict, kind: str, steps: int, every: int, pattern: str = "ab"):
+def run_case(case: dict, kind: str, steps: int, every: int, pattern: str = "ab", fast: bool = False):
     c = dict(case)
     c["kind"] = kind
     scale = 256.0 if kind == "f16" else 1.0
-    lat = CS.make_lattice(c, pattern=pattern, scale=scale)
+    lat = CS.make_lattice(c, pattern=pattern, scale=scale, fast=fast)
     nodes = c["l"] * c["m"] * c["n"]
     series = []
     t0 = time.perf_counter()
@@ -93,7 +93,7 @@ def run_case(case: dict, kind: str, steps: int, every: int, pattern: str = "ab")
     if CS.obstacle_mask(c) is not None:
         fluid = torch.from_numpy(CS.obstacle_mask(c) != 1).to(lat.device)
     lat.close()
-    return {"kind": kind, "series": series, "u": u, "rho": rho, "fluid": fluid, "wall_s": wall,
+    return {"kind": kind, "mode": "fast" if fast else "strict", "series": series, "u": u, "rho": rho, "fluid": fluid, "wall_s": wall,
             "glups_incl_diag": nodes * steps / wall / 1e9}
 
 
@@ -106,7 +106,7 @@ def compare(ref, got):
         rb = b if fl is None else b[fl]
         num += float(torch.sum(diff * diff))
         den += float(torch.sum(rb * rb))
-    out = {"kind": got["kind"], "l2_velocity_rel": (num / den) ** 0.5}
+    out = {"kind": got["kind"], "mode": got["mode"], "l2_velocity_rel": (num / den) ** 0.5}
     ke_ref = np.array([r["ke"] for r in ref["series"]])
     ke = np.array([r["ke"] for r in got["series"]])
     out["ke_rel_max"] = float(np.max(np.abs(ke - ke_ref) / np.abs(ke_ref)))
@@ -136,6 +136,9 @@ def main(argv=None):
     ap.add_argument("--every", type=int, default=10)
     ap.add_argument("--kinds", default="f32,f16,bf16")
     ap.add_argument("--pattern", default="ab")
+    ap.add_argument("--modes", default="strict",
+                    help="collision of the compared kinds: strict (reference order), fast (fused "
+                         "multiply-add) or both (strict,fast); the FP64 reference is always strict")
     ap.add_argument("--size", type=int, nargs="*", default=None)
     args = ap.parse_args(argv)
     if args.case == "tgv":
@@ -153,12 +156,15 @@ def main(argv=None):
                       **({"drag_final": ref["series"][-1]["drag"]} if "drag" in ref["series"][-1] else {}),
                       "glups_incl_diag": ref["glups_incl_diag"]}), flush=True)
     for kind in args.kinds.split(","):
-        got = run_case(case, kind, args.steps, args.every, args.pattern)
-        res = compare(ref, got)
-        res.update({"case": case["name"].rsplit("_", 1)[0], "steps": args.steps, "every": args.every})
-        print(json.dumps(res), flush=True)
-        del got
-        torch.cuda.empty_cache()
+        for mode in args.modes.split(","):
+            if mode == "fast" and kind in ("f64", "f32_f64"):
+                continue        # fused collision: float compute only
+            got = run_case(case, kind, args.steps, args.every, args.pattern, fast=(mode == "fast"))
+            res = compare(ref, got)
+            res.update({"case": case["name"].rsplit("_", 1)[0], "steps": args.steps, "every": args.every})
+            print(json.dumps(res), flush=True)
+            del got
+            torch.cuda.empty_cache()
     return 0
 
 
