@@ -56,7 +56,7 @@ long long sweep_blocks(const bgk_sweep_params* p, const void* a0) {
 }
 
 int finalize_moments(const double* partials, long long nparts, double* out, cudaStream_t st) {
-    finalize_partials_kernel<5><<<1, 256, 0, st>>>(partials, nparts, out);
+    finalize_partials_kernel<5><<<1, kFinalizeThreads, 0, st>>>(partials, nparts, out);
     return check_launch("finalize_partials_kernel");
 }
 

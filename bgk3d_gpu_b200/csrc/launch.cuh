@@ -247,7 +247,7 @@ int launch_moments(const bgk_sweep_params* p, void* const* a, double* out, doubl
     moments_partial_kernel<S, C><<<grd, blk, 0, st>>>(F, ws);
     if (int e = check_launch("moments_partial_kernel")) return e;
     const long long nparts = (long long)grd.x * grd.y * grd.z;
-    finalize_partials_kernel<5><<<1, 256, 0, st>>>(ws, nparts, out);
+    finalize_partials_kernel<5><<<1, kFinalizeThreads, 0, st>>>(ws, nparts, out);
     return check_launch("finalize_partials_kernel");
 }
 
@@ -262,7 +262,7 @@ int launch_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, i
         return set_error(BGK_ERR_ARG, "draglift box needs %lld bytes of workspace", nb * 3 * 8);
     draglift_partial_kernel<S, C><<<(unsigned)nb, 256, 0, st>>>(F, is, js, ks, ni, nj, nk, ws);
     if (int e = check_launch("draglift_partial_kernel")) return e;
-    finalize_partials_kernel<3><<<1, 256, 0, st>>>(ws, nb, out);
+    finalize_partials_kernel<3><<<1, kFinalizeThreads, 0, st>>>(ws, nb, out);
     return check_launch("finalize_partials_kernel");
 }
 

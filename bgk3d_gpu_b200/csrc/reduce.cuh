@@ -128,28 +128,51 @@ __global__ void __launch_bounds__(256) draglift_partial_kernel(const FieldArgs<S
 }
 
 // Second pass: one block sums nparts partials of NQ values in a fixed order.
+// Thread t adds partials t, t + T, t + 2T, ... in that order (T = 1024), four
+// loads in flight at a time (a partial array of the fused-moments sweep at
+// 256^3 holds ~74 K records: one strided load at a time per thread made this
+// pass ~0.2 ms, as long as the sweep); then the threads' sums are combined
+// by a fixed shuffle tree and the warps' in warp order.
+constexpr int kFinalizeThreads = 1024;
 template <int NQ>
-__global__ void __launch_bounds__(256) finalize_partials_kernel(const double* partial, long long nparts,
-                                                                double* out) {
-    __shared__ double sm[256][NQ];
+__global__ void __launch_bounds__(kFinalizeThreads) finalize_partials_kernel(const double* partial, long long nparts,
+                                                                             double* out) {
+    constexpr int T = kFinalizeThreads, U = 4;
+    __shared__ double sm[T / 32][NQ];
     double v[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) v[q] = 0.0;
-    for (long long p = threadIdx.x; p < nparts; p += blockDim.x)
+    long long p = threadIdx.x;
+    for (; p + (U - 1) * (long long)T < nparts; p += U * (long long)T) {
+        double t[U][NQ];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) t[u][q] = partial[(p + u * (long long)T) * NQ + q];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) v[q] += t[u][q];
+    }
+    for (; p < nparts; p += T)
 #pragma unroll
         for (int q = 0; q < NQ; ++q) v[q] += partial[p * NQ + q];
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) sm[threadIdx.x][q] = v[q];
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s)
+    for (int q = 0; q < NQ; ++q)
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) sm[threadIdx.x][q] += sm[threadIdx.x + s][q];
-        __syncthreads();
-    }
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) sm[warp][q] = v[q];
+    __syncthreads();
     if (threadIdx.x == 0)
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) out[q] = sm[0][q];
+        for (int q = 0; q < NQ; ++q) {
+            double s2 = 0.0;
+            for (int w = 0; w < T / 32; ++w) s2 += sm[w][q];
+            out[q] = s2;
+        }
 }
 
 }  // namespace bgk
