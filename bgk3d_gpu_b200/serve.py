@@ -56,6 +56,7 @@ class Request:
     steps: int
     tau: float
     kind: str               # "f32" | "f16"
+    fast: bool = False      # fused-multiply-add collision (same stated accuracy, see accuracy.py)
 
 
 def make_trace(n: int, rate: float = 50.0, seed: int = 7, side_range=(32, 256), step_range=(500, 10000)):
@@ -111,7 +112,7 @@ class _Active:
     def __init__(self, req: Request, t_admit: float):
         self.req = req
         self.case = case_of(req)
-        self.lat = CS.make_lattice(self.case)
+        self.lat = CS.make_lattice(self.case, fast=req.fast)
         self.remaining = req.steps
         self.t_admit = t_admit
         self.bytes = self.lat.device_bytes
@@ -260,12 +261,17 @@ def main(argv=None):
     ap.add_argument("--modes", default="continuous,shared,fifo,plain")
     ap.add_argument("--floor-nodes", type=float, default=8e6)
     ap.add_argument("--alone-nodes", type=float, default=2e6)
+    ap.add_argument("--fast", action="store_true",
+                    help="solve every request with the fused-multiply-add collision (FP16 requests then take "
+                         "the two-node sweep; L2 velocity error unchanged at the FP16 storage level)")
     ap.add_argument("--max-side", type=int, default=256)
     ap.add_argument("--max-steps", type=int, default=10000)
     args = ap.parse_args(argv)
     trace = make_trace(args.requests, args.rate, args.seed, side_range=(32, args.max_side),
                        step_range=(500, args.max_steps))
-    out = {"trace": {"requests": args.requests, "rate_per_s": args.rate, "seed": args.seed,
+    for r in trace:
+        r.fast = args.fast
+    out = {"trace": {"requests": args.requests, "rate_per_s": args.rate, "seed": args.seed, "fast": args.fast,
                      "side": [32, args.max_side], "steps": [500, args.max_steps],
                      "total_lups": sum(r.side ** 3 * (2 if r.case == "sphere" else 1) * r.steps for r in trace)}}
     for mode in args.modes.split(","):

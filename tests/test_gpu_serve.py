@@ -7,9 +7,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _trace():
+def _trace(fast=False):
     from bgk3d_gpu_b200.serve import Request
-    return [
+    reqs = [
         Request(0, 0.00, "ldc", 24, 90, 0.6, "f32"),
         Request(1, 0.00, "tgv", 32, 40, 0.55, "f32"),
         Request(2, 0.01, "sphere", 32, 65, 0.52, "f32"),
@@ -17,13 +17,16 @@ def _trace():
         Request(4, 0.02, "ldc", 20, 33, 0.8, "f16"),
         Request(5, 0.05, "sphere", 24, 17, 0.6, "f16"),
     ]
+    for r in reqs:
+        r.fast = fast
+    return reqs
 
 
 def _alone(req):
     from bgk3d_gpu_b200 import cases as CS
     from bgk3d_gpu_b200.serve import case_of
     c = case_of(req)
-    lat = CS.make_lattice(c)
+    lat = CS.make_lattice(c, fast=req.fast)
     lat.step(req.steps)
     st = lat.download()
     m = lat.moments()
@@ -31,12 +34,15 @@ def _alone(req):
     return st, m
 
 
-@pytest.mark.parametrize("mode,floor", [("continuous", 8e6), ("continuous", 3e4), ("shared", 0)])
-def test_results_identical_alone_and_in_the_mix(mode, floor):
+@pytest.mark.parametrize("mode,floor,fast", [("continuous", 8e6, False), ("continuous", 3e4, False),
+                                             ("shared", 0, False), ("continuous", 3e4, True)])
+def test_results_identical_alone_and_in_the_mix(mode, floor, fast):
     """floor 3e4 nodes makes the shortest-work-first policy step only a few
-    solves per round, so batches change membership between rounds."""
+    solves per round, so batches change membership between rounds.  With the
+    fused collision the FP16 requests step alone through the two-node sweep
+    and in the mix through the batched one-node sweep: still bit-identical."""
     from bgk3d_gpu_b200.serve import Server
-    trace = _trace()
+    trace = _trace(fast)
     done, summary = Server(budget_bytes=20e9, max_chunk=25, floor_nodes=floor).run(trace, mode=mode,
                                                                                  keep_states=True)
     assert summary["requests"] == len(trace)
