@@ -284,6 +284,20 @@ int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* m
     if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
     const unsigned blocks = (unsigned)((warps + 7) / 8);
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
+    if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
+        const int cm = coll_mode(A);
+        if (!odd && g_pair_kernels && cm_fast(cm) && A.obs == nullptr && mom == nullptr &&
+            p->bcase != BC_INFLOW && nelem < (1LL << 31) && pairs_aligned<S>(p, slots, slots)) {
+            SweepArgs<S, C> A2 = A;
+            A2.nseg = (p->l + 63) / 64;
+            A2.div_seg.init((uint32_t)A2.nseg);
+            constexpr int wpb = kPairThreads / 32;
+            const unsigned nb2 = (unsigned)(((long long)A2.nseg * p->m * p->n + wpb - 1) / wpb);
+            if (cm == CM_FAST) aa_even_pair_kernel<S, C, CM_FAST><<<nb2, kPairThreads, 0, st>>>(A2);
+            else aa_even_pair_kernel<S, C, CM_FAST_GENERIC><<<nb2, kPairThreads, 0, st>>>(A2);
+            return check_launch("aa_even_pair_kernel");
+        }
+    }
     switch (p->bcase) {
         case BC_DRIVEN: launch_aa_bc<S, C, BC_DRIVEN>(A, odd, nelem, blocks, st); break;
         case BC_PERIODIC: launch_aa_bc<S, C, BC_PERIODIC>(A, odd, nelem, blocks, st); break;

@@ -61,18 +61,19 @@ __device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, double (&
     if (OBS && P.obs != nullptr && i >= P.imin && i <= P.imax && j >= P.jmin && j <= P.jmax &&
         k >= P.kmin && k <= P.kmax && (obstacle_links(P, i, j, k) & 0x80000000u))
         return;
-    S** f = const_cast<S**>(P.a);
+    // the slot arrays: read through P.a, written through P.b (the same arrays;
+    // indexing the kernel parameters directly keeps them out of local memory)
     const float inv = P.inv_scale;
     C x[19];
 #pragma unroll
-    for (int d = 0; d < 19; ++d) x[d] = Conv<S, C>::raw(f[d][c]);
+    for (int d = 0; d < 19; ++d) x[d] = Conv<S, C>::raw(P.a[d][c]);
     C y[19];
     collide_cm<S, C, CM>(x, y, P.col, P.fc, inv);
     S st[19];
 #pragma unroll
     for (int d = 0; d < 19; ++d) st[d] = Conv<S, C>::pack(y[d]);
 #pragma unroll
-    for (int d = 0; d < 19; ++d) f[opp_of(d)][c] = st[d];
+    for (int d = 0; d < 19; ++d) P.b[opp_of(d)][c] = st[d];
     if (BC == BC_INFLOW && i == P.l) {
         C s[19];
 #pragma unroll
@@ -80,7 +81,7 @@ __device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, double (&
         C eq[5];
         outflow_eq<C, Scaled<S>::value>(s, P.inflow_cte1, P.col, inv, eq);
 #pragma unroll
-        for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::pack(eq[e]);
+        for (int e = 0; e < 5; ++e) P.b[opp_of(9 + e)][c + 1] = Conv<S, C>::pack(eq[e]);
     }
     if (P.mom != nullptr) {
         C s[19];
@@ -97,6 +98,37 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(co
     if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 
+// Even step of the 16-bit kinds with the fused collision on aligned pairs
+// (the adjacent-pair layout of sweep_abp_kernel): thread t reads the 19 slot
+// words of its pair (i, i + 1), runs the two collisions as one on packed
+// FP32 pairs and writes population p of both nodes as one word into slot
+// opp(p); bit-identical to aa_even_kernel.  Purely local, so no shuffles.
+// No obstacle, no fused moments, not the inflow case (whose node l also
+// writes the outflow halo); the host takes aa_even_kernel for those.
+template <class S, class C, int CM>
+__global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel(const SweepArgs<S, C> P) {
+    static_assert(sizeof(S) == 2 && sizeof(C) == 4 && cm_fast(CM), "pair step: 16-bit storage, fused collision");
+    const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const uint32_t row = P.div_seg.div(gw);
+    if (row >= P.nrows) return;
+    const int seg = (int)(gw - row * (uint32_t)P.nseg);
+    const uint32_t kk = P.div_m.div(row);
+    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
+    const int k = (int)kk + 1;
+    const int i0 = seg * 64 + 2 * lane + 1;
+    if (i0 >= P.l) return;                            // l even: the pair (i0, i0 + 1) is inside
+    const int c = (int)P.nx * j + (int)P.nxy * k + i0;
+    // P.a and P.b name the same slot arrays (P.b[18] too)
+    uint32_t wv[19];
+#pragma unroll
+    for (int d = 0; d < 19; ++d) wv[d] = *reinterpret_cast<const unsigned*>(P.a[d] + c);   // all reads first
+    auto xs = [&](int d) { return raw_bits<S>(wv[d]); };
+    auto xp = [&](int d) { return raw_bits_again<S>(wv[d]); };
+    auto ys = [&](int d, F2 y) { *reinterpret_cast<unsigned*>(P.b[opp_of(d)] + c) = pack_bits<S>(y); };
+    bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
+}
+
 // Odd (pull + push) step.
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
@@ -110,7 +142,8 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
         sl = obstacle_links(P, i, j, k);
         if (sl & 0x80000000u) return;
     }
-    S** f = const_cast<S**>(P.a);
+    // the slot arrays: read through P.a, written through P.b (the same arrays;
+    // indexing the kernel parameters directly keeps them out of local memory)
     const IDX nx = (IDX)P.nx, nxy = (IDX)P.nxy;
     // offset of the neighbour at -1 / +1 along each axis (periodic axes wrap)
     const IDX oxm = (F::PX && i == 1) ? (IDX)(P.l - 1) : (IDX)(-1);
@@ -137,14 +170,14 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
         if (cx == 1) bounce |= wxm; else if (cx == -1) bounce |= wxp;
         if (cy == 1) bounce |= wym; else if (cy == -1) bounce |= wyp;
         if (cz == 1) bounce |= wzm; else if (cz == -1) bounce |= wzp;
-        C v = Conv<S, C>::raw(bounce ? f[d][c] : f[opp_of(d)][off]);
+        C v = Conv<S, C>::raw(bounce ? P.a[d][c] : P.a[opp_of(d)][off]);
         if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
             v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force);
         if (BC == BC_INFLOW && cx == 1 && i == 1)
             v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
         x[d] = v;
     }
-    x[18] = Conv<S, C>::raw(f[18][c]);
+    x[18] = Conv<S, C>::raw(P.a[18][c]);
     C y[19];
     collide_cm<S, C, CM>(x, y, P.col, P.fc, inv);
     S sv[19];
@@ -168,13 +201,13 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
                 const C r = Conv<S, C>::raw(sv[d]);
                 bv = Conv<S, C>::pack(od == 1 ? r + P.lid_force : r - P.lid_force);
             }
-            f[od][c] = bv;
+            P.b[od][c] = bv;
         } else {
             const bool gone = BC == BC_INFLOW && ((cx == -1 && i == 1) || (cx == 1 && i == P.l));
-            if (!gone) f[d][off] = sv[d];
+            if (!gone) P.b[d][off] = sv[d];
         }
     }
-    f[18][c] = sv[18];
+    P.b[18][c] = sv[18];
     if (P.mom != nullptr) {
         C s[19];
 #pragma unroll
@@ -184,7 +217,7 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
     if (BC == BC_INFLOW && i == 1) {
 #pragma unroll
         for (int d = 0; d < 5; ++d)
-            f[d][c] = Conv<S, C>::pack(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
+            P.b[d][c] = Conv<S, C>::pack(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
     }
     if (BC == BC_INFLOW && i == P.l) {
         C s[19];
@@ -198,7 +231,7 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
             IDX off = c;   // (l+1, j, k) + c_d = (l, j + c_y, k + c_z)
             if (cy == 1) off += oyp; else if (cy == -1) off += oym;
             if (cz == 1) off += ozp; else if (cz == -1) off += ozm;
-            f[d][off] = Conv<S, C>::pack(eq[e]);
+            P.b[d][off] = Conv<S, C>::pack(eq[e]);
         }
     }
 }
@@ -217,15 +250,16 @@ __global__ void aa_outflow_prepass_kernel(const SweepArgs<S, C> P) {
     const int j = 1 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int k = 1 + (int)blockIdx.y;
     if (j > P.m) return;
-    S** f = const_cast<S**>(P.a);
+    // the slot arrays: read through P.a, written through P.b (the same arrays;
+    // indexing the kernel parameters directly keeps them out of local memory)
     const long long c = (long long)P.l + P.nx * (long long)j + P.nxy * (long long)k;
     C s[19];
 #pragma unroll
-    for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::raw(f[opp_of(d)][c]);
+    for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::raw(P.a[opp_of(d)][c]);
     C eq[5];
     outflow_eq<C, Scaled<S>::value>(s, P.inflow_cte1, P.col, P.inv_scale, eq);
 #pragma unroll
-    for (int e = 0; e < 5; ++e) f[opp_of(9 + e)][c + 1] = Conv<S, C>::pack(eq[e]);
+    for (int e = 0; e < 5; ++e) P.b[opp_of(9 + e)][c + 1] = Conv<S, C>::pack(eq[e]);
 }
 
 }  // namespace bgk

@@ -93,15 +93,15 @@ def main(argv=None) -> int:
                         if tma == "on" and pattern == "aa":
                             continue    # the TMA sweep serves AB lattices
                         for pair in args.pair.split(","):
-                            if pair == "off" and (BYTES[kind] != 2 or pattern == "aa" or tma == "on"):
-                                continue    # the two-node sweep serves 16-bit AB lattices
+                            if pair == "off" and (BYTES[kind] != 2 or tma == "on"):
+                                continue    # the two-node sweeps serve 16-bit lattices
                             prev = lib().bgk_set_tma_kernels(1 if tma == "on" else 0)
                             prev_pair = lib().bgk_set_pair_kernels(1 if pair == "on" else 0)
                             lat = make(kind, pattern, case, l, m, n, fast=(mode == "fast"))
                             if lat.L.bgk_lattice_uses_tma(lat.h):
                                 path = "tma"
-                            elif pair == "on" and BYTES[kind] == 2 and pattern == "ab" and case != "inflow" and mode == "fast":
-                                path = "two-node"
+                            elif pair == "on" and BYTES[kind] == 2 and case != "inflow" and mode == "fast":
+                                path = "two-node" if pattern == "ab" else "two-node even step"
                             else:
                                 path = "one-node"
                             s = time_steps(lat, args.steps, args.warmup)

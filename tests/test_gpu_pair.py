@@ -4,7 +4,8 @@ collision) against the one-node sweep: bit-identical states for FP16 and
 BF16 storage, every boundary case, force-free and forced collisions, on
 library-owned lattices (aligned rows) and on the reference layout with odd
 paddings (rows starting anywhere in a segment), with row lengths that leave
-partial 64-node segments."""
+partial 64-node segments; and the even step of the in-place AA pattern in
+pairs (aa_even_pair_kernel)."""
 import zlib
 
 import numpy as np
@@ -23,14 +24,14 @@ def _switch(on: bool) -> int:
     return lib().bgk_set_pair_kernels(1 if on else 0)
 
 
-def _lattice(kind, case, shape, fast, on, steps=5):
+def _lattice(kind, case, shape, fast, on, steps=5, pattern="ab"):
     from bgk3d_gpu_b200.lattice import Lattice
     l, m, n = shape
     p = CASE_PARAMS[case]
     prev = _switch(on)
     try:
         lat = Lattice(l, m, n, kind=kind, bcase=BCASE[case], omega=OMEGA, scale=SCALE[kind], fast=fast,
-                      lid_force=p.get("lid_force", 0.0), u_inflow=p.get("u_inflow", 0.0),
+                      pattern=pattern, lid_force=p.get("lid_force", 0.0), u_inflow=p.get("u_inflow", 0.0),
                       force_mode=p.get("force_mode", 0), force=p.get("force", (0.0, 0.0, 0.0)))
         seed = zlib.crc32(repr((kind, case, shape)).encode()) % 1000
         lat.upload(random_state(l, m, n, kind, seed=seed, scale=SCALE[kind]))
@@ -77,6 +78,18 @@ def test_pair_equals_one_node_sweep_on_reference_layout(kind, case, ipad, jpad):
         b = _reference_layout(kind, case, shape, True, False, ipad, jpad)
         bad = np.argwhere(a != b)
         assert len(bad) == 0, (kind, case, shape, ipad, len(bad), bad[:5].tolist())
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+@pytest.mark.parametrize("case", [c for c in CASES if c != "none"])
+def test_aa_even_pair_step_equals_one_node_step(kind, case):
+    """The in-place pattern: even steps through aa_even_pair_kernel, odd steps
+    through aa_odd_kernel, against both through the one-node kernels."""
+    for shape in SHAPES:
+        a = _lattice(kind, case, shape, True, True, steps=6, pattern="aa")
+        b = _lattice(kind, case, shape, True, False, steps=6, pattern="aa")
+        bad = np.argwhere(a != b)
+        assert len(bad) == 0, (kind, case, shape, len(bad), bad[:5].tolist())
 
 
 def test_pair_switch_default_on():
