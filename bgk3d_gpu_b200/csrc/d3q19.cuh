@@ -154,93 +154,81 @@ __host__ __device__ constexpr bool cm_fast(int cm) { return cm >= 2; }
 // cte0 = 0) without forcing: it omits the terms that are then additions of
 // +0 or multiplications by 1, which changes no result except possibly the
 // sign of an exact zero.
-template <class V, class C, bool GENERIC, bool SCALED>
-__device__ __forceinline__ void bgk_collide_v(const V (&x)[19], V (&y)[19], const ColConst<C>& P, float inv) {
+//
+// bgk_collide_f reads population d through xs(d) for the moment sums and
+// through xp(d) for the relaxation, and hands y_d to ys(d, y_d); the
+// equilibria are formed pair by pair (+-c share their velocity term), so
+// that a caller short of registers never holds all 19 of them.  Every value
+// is computed by the same operations in the same order as in the reference.
+template <class V, class C, bool GENERIC, bool SCALED, class XS, class XP, class YS>
+__device__ __forceinline__ void bgk_collide_f(XS xs, XP xp, YS ys, const ColConst<C>& P, float inv) {
     const V cte0 = V(P.cte0), cte1 = V(P.cte1), tre = V(P.tre), qf = V(P.qf), rf = V(P.rf);
-    V sum = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] +
-            x[11] + x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18];
+    V sum = xs(0) + xs(1) + xs(2) + xs(3) + xs(4) + xs(5) + xs(6) + xs(7) + xs(8) + xs(9) + xs(10) +
+            xs(11) + xs(12) + xs(13) + xs(14) + xs(15) + xs(16) + xs(17) + xs(18);
     if (SCALED) sum = sum * V((C)inv);
     const V rho = sum + cte1;
     const V rhoinv = V(C(1)) / rho;
-    V mx = x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13];
-    V my = x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17];
-    V mz = x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15];
+    V mx = xs(0) + xs(1) + xs(2) + xs(3) + xs(4) - xs(9) - xs(10) - xs(11) - xs(12) - xs(13);
+    V my = xs(2) + xs(6) + xs(7) + xs(8) + xs(11) - xs(0) - xs(9) - xs(15) - xs(16) - xs(17);
+    V mz = xs(3) + xs(5) + xs(6) + xs(12) + xs(17) - xs(1) - xs(8) - xs(10) - xs(14) - xs(15);
     if (SCALED) { mx = mx * V((C)inv); my = my * V((C)inv); mz = mz * V((C)inv); }
-    V vx = mx * rhoinv, vy = my * rhoinv, vz = mz * rhoinv;
+    const V vx = mx * rhoinv, vy = my * rhoinv, vz = mz * rhoinv;
     const V vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
     const V vsq = vx2 + vy2 + vz2;
     auto q = [&](V t) -> V { return GENERIC ? cte0 + qf * t : qf * t; };
-    V vxpy = vx + vy;
-    const V qxpy = q(tre * vxpy * vxpy - vsq);
-    V vxmy = vx - vy;
-    const V qxmy = q(tre * vxmy * vxmy - vsq);
-    V vxpz = vx + vz;
-    const V qxpz = q(tre * vxpz * vxpz - vsq);
-    V vxmz = vx - vz;
-    const V qxmz = q(tre * vxmz * vxmz - vsq);
-    V vypz = vy + vz;
-    const V qypz = q(tre * vypz * vypz - vsq);
-    V vymz = vy - vz;
-    const V qymz = q(tre * vymz * vymz - vsq);
-    const V qx = q(tre * vx2 - vsq);
-    const V qy = q(tre * vy2 - vsq);
-    const V qz = q(tre * vz2 - vsq);
-    const V q0 = q(-vsq);
-    vx = rf * vx; vy = rf * vy; vz = rf * vz;
-    vxpy = rf * vxpy; vxmy = rf * vxmy; vxpz = rf * vxpz;
-    vxmz = rf * vxmz; vypz = rf * vypz; vymz = rf * vymz;
     const V p0 = V(P.p0), p1 = V(P.p1), p2 = V(P.p2);
     const V rp0 = rho * p0, rp1 = rho * p1, rp2 = rho * p2;
     const V s2 = GENERIC ? cte1 * (rp2 - p2) : rp2 - p2;
     const V s1 = GENERIC ? cte1 * (rp1 - p1) : rp1 - p1;
     const V s0 = GENERIC ? cte1 * (rp0 - p0) : rp0 - p0;
-    V e[19];
-    e[0] = rp2 * (+vxmy + qxmy) + s2;
-    e[1] = rp2 * (+vxmz + qxmz) + s2;
-    e[2] = rp2 * (+vxpy + qxpy) + s2;
-    e[3] = rp2 * (+vxpz + qxpz) + s2;
-    e[4] = rp1 * (+vx + qx) + s1;
-    e[5] = rp1 * (+vz + qz) + s1;
-    e[6] = rp2 * (+vypz + qypz) + s2;
-    e[7] = rp1 * (+vy + qy) + s1;
-    e[8] = rp2 * (+vymz + qymz) + s2;
-    e[9] = rp2 * (-vxpy + qxpy) + s2;
-    e[10] = rp2 * (-vxpz + qxpz) + s2;
-    e[11] = rp2 * (-vxmy + qxmy) + s2;
-    e[12] = rp2 * (-vxmz + qxmz) + s2;
-    e[13] = rp1 * (-vx + qx) + s1;
-    e[14] = rp1 * (-vz + qz) + s1;
-    e[15] = rp2 * (-vypz + qypz) + s2;
-    e[16] = rp1 * (-vy + qy) + s1;
-    e[17] = rp2 * (-vymz + qymz) + s2;
-    e[18] = rp0 * (+q0) + s0;
     const V om = V(P.omega);
-    if (!GENERIC) {
-#pragma unroll
-        for (int d = 0; d < 18; ++d) y[d] = x[d] - om * (x[d] - e[d]);
-    } else {
-    V fx = V(P.fx), fy = V(P.fy), fz = V(P.fz);
-    if (P.force_mode == 1) { fx = V(P.fx) * rho; fy = V(P.fy) * rho; fz = V(P.fz) * rho; }
-    y[0] = x[0] - om * (x[0] - e[0]) + fx - fy;
-    y[1] = x[1] - om * (x[1] - e[1]) + fx - fz;
-    y[2] = x[2] - om * (x[2] - e[2]) + fx + fy;
-    y[3] = x[3] - om * (x[3] - e[3]) + fx + fz;
-    y[4] = x[4] - om * (x[4] - e[4]) + fx;
-    y[5] = x[5] - om * (x[5] - e[5]) + fz;
-    y[6] = x[6] - om * (x[6] - e[6]) + fy + fz;
-    y[7] = x[7] - om * (x[7] - e[7]) + fy;
-    y[8] = x[8] - om * (x[8] - e[8]) + fy - fz;
-    y[9] = x[9] - om * (x[9] - e[9]) - fx - fy;
-    y[10] = x[10] - om * (x[10] - e[10]) - fx - fz;
-    y[11] = x[11] - om * (x[11] - e[11]) - fx + fy;
-    y[12] = x[12] - om * (x[12] - e[12]) - fx + fz;
-    y[13] = x[13] - om * (x[13] - e[13]) - fx;
-    y[14] = x[14] - om * (x[14] - e[14]) - fz;
-    y[15] = x[15] - om * (x[15] - e[15]) - fy - fz;
-    y[16] = x[16] - om * (x[16] - e[16]) - fy;
-    y[17] = x[17] - om * (x[17] - e[17]) - fy + fz;
+    V fx = V(C(0)), fy = V(C(0)), fz = V(C(0));
+    if (GENERIC) {
+        fx = V(P.fx); fy = V(P.fy); fz = V(P.fz);
+        if (P.force_mode == 1) { fx = V(P.fx) * rho; fy = V(P.fy) * rho; fz = V(P.fz) * rho; }
     }
-    y[18] = x[18] - om * (x[18] - e[18]);
+    // relaxation of population d towards its equilibrium e
+    auto relax = [&](int d, V e) -> V { return xp(d) - om * (xp(d) - e); };
+    // axis pair dp / dm along v_a: q from tre (v_a v_a); force +-f
+    auto axis = [&](int dp, int dm, V v, V v2, V f) {
+        const V qa = q(tre * v2 - vsq);
+        const V lin = rf * v;
+        const V yp = relax(dp, rp1 * (+lin + qa) + s1), ym = relax(dm, rp1 * (-lin + qa) + s1);
+        ys(dp, GENERIC ? yp + f : yp);
+        ys(dm, GENERIC ? ym - f : ym);
+    };
+    // diagonal pair dp / dm along v = v_a +- v_b: q from (tre v) v; forces
+    // added one at a time as the reference writes them, dp: + fa +- fb,
+    // dm: - fa -+ fb (bminus: the sign of fb in dp is minus)
+    auto diag = [&](int dp, int dm, V v, V fa, V fb, bool bminus) {
+        const V qd = q(tre * v * v - vsq);
+        const V lin = rf * v;
+        const V yp = relax(dp, rp2 * (+lin + qd) + s2), ym = relax(dm, rp2 * (-lin + qd) + s2);
+        if (GENERIC) {
+            const V yp1 = yp + fa, ym1 = ym - fa;
+            ys(dp, bminus ? yp1 - fb : yp1 + fb);
+            ys(dm, bminus ? ym1 + fb : ym1 - fb);
+        } else {
+            ys(dp, yp);
+            ys(dm, ym);
+        }
+    };
+    diag(0, 11, vx - vy, fx, fy, true);
+    diag(1, 12, vx - vz, fx, fz, true);
+    diag(2, 9, vx + vy, fx, fy, false);
+    diag(3, 10, vx + vz, fx, fz, false);
+    axis(4, 13, vx, vx2, fx);
+    axis(5, 14, vz, vz2, fz);
+    diag(6, 15, vy + vz, fy, fz, false);
+    axis(7, 16, vy, vy2, fy);
+    diag(8, 17, vy - vz, fy, fz, true);
+    ys(18, relax(18, rp0 * (+q(-vsq)) + s0));
+}
+
+template <class V, class C, bool GENERIC, bool SCALED>
+__device__ __forceinline__ void bgk_collide_v(const V (&x)[19], V (&y)[19], const ColConst<C>& P, float inv) {
+    auto xr = [&](int d) { return x[d]; };
+    bgk_collide_f<V, C, GENERIC, SCALED>(xr, xr, [&](int d, V v) { y[d] = v; }, P, inv);
 }
 
 // The collision on one node's compute values.

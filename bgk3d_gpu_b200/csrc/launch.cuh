@@ -66,7 +66,7 @@ template <class S, class C, int BC, class IDX, int CM, bool OBS> struct Ab2Launc
 };
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbpLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
-        if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && !OBS && sizeof(IDX) == 4 && cm_fast(CM))
+        if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && !OBS && sizeof(IDX) == 4)
             sweep_abp_kernel<S, C, BC, CM><<<blocks, kPairThreads, 0, st>>>(A);
     }
 };
@@ -116,8 +116,7 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     const bool obs = A.obs != nullptr;
     const unsigned nb = (unsigned)blocks;
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
-        if (g_pair_kernels && cm_fast(cm) && !obs && mom == nullptr && nelem < (1LL << 31) &&
-            pairs_aligned<S>(p, a, b)) {
+        if (g_pair_kernels && !obs && mom == nullptr && nelem < (1LL << 31) && pairs_aligned<S>(p, a, b)) {
             // adjacent node pairs: 64-node segments from i = 1
             SweepArgs<S, C> A2 = A;
             A2.nseg = (p->l + 63) / 64;
@@ -286,15 +285,21 @@ int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* m
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
         const int cm = coll_mode(A);
-        if (!odd && g_pair_kernels && cm_fast(cm) && A.obs == nullptr && mom == nullptr &&
+        if (!odd && g_pair_kernels && A.obs == nullptr && mom == nullptr &&
             p->bcase != BC_INFLOW && nelem < (1LL << 31) && pairs_aligned<S>(p, slots, slots)) {
             SweepArgs<S, C> A2 = A;
             A2.nseg = (p->l + 63) / 64;
             A2.div_seg.init((uint32_t)A2.nseg);
             constexpr int wpb = kPairThreads / 32;
             const unsigned nb2 = (unsigned)(((long long)A2.nseg * p->m * p->n + wpb - 1) / wpb);
-            if (cm == CM_FAST) aa_even_pair_kernel<S, C, CM_FAST><<<nb2, kPairThreads, 0, st>>>(A2);
-            else aa_even_pair_kernel<S, C, CM_FAST_GENERIC><<<nb2, kPairThreads, 0, st>>>(A2);
+            switch (cm) {
+                case CM_STRICT: aa_even_pair_kernel<S, C, CM_STRICT><<<nb2, kPairThreads, 0, st>>>(A2); break;
+                case CM_STRICT_GENERIC:
+                    aa_even_pair_kernel<S, C, CM_STRICT_GENERIC><<<nb2, kPairThreads, 0, st>>>(A2);
+                    break;
+                case CM_FAST: aa_even_pair_kernel<S, C, CM_FAST><<<nb2, kPairThreads, 0, st>>>(A2); break;
+                default: aa_even_pair_kernel<S, C, CM_FAST_GENERIC><<<nb2, kPairThreads, 0, st>>>(A2); break;
+            }
             return check_launch("aa_even_pair_kernel");
         }
     }

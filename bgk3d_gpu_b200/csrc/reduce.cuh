@@ -128,12 +128,13 @@ __global__ void __launch_bounds__(256) draglift_partial_kernel(const FieldArgs<S
 }
 
 // Second pass: one block sums nparts partials of NQ values in a fixed order.
-// Thread t adds partials t, t + T, t + 2T, ... in that order (T = 1024), four
-// loads in flight at a time (a partial array of the fused-moments sweep at
+// Thread t adds partials t, t + T, t + 2T, ... in that order (T = 512, so
+// that the four records in flight fit in registers), four loads in flight at
+// a time (a partial array of the fused-moments sweep at
 // 256^3 holds ~74 K records: one strided load at a time per thread made this
 // pass ~0.2 ms, as long as the sweep); then the threads' sums are combined
 // by a fixed shuffle tree and the warps' in warp order.
-constexpr int kFinalizeThreads = 1024;
+constexpr int kFinalizeThreads = 512;
 template <int NQ>
 __global__ void __launch_bounds__(kFinalizeThreads) finalize_partials_kernel(const double* partial, long long nparts,
                                                                              double* out) {

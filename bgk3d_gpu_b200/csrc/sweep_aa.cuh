@@ -98,16 +98,17 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(co
     if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
 }
 
-// Even step of the 16-bit kinds with the fused collision on aligned pairs
+// Even step of the 16-bit kinds on aligned pairs
 // (the adjacent-pair layout of sweep_abp_kernel): thread t reads the 19 slot
 // words of its pair (i, i + 1), runs the two collisions as one on packed
 // FP32 pairs and writes population p of both nodes as one word into slot
-// opp(p); bit-identical to aa_even_kernel.  Purely local, so no shuffles.
+// opp(p); bit-identical to aa_even_kernel, in either collision mode.  Purely
+// local, so no shuffles.
 // No obstacle, no fused moments, not the inflow case (whose node l also
 // writes the outflow halo); the host takes aa_even_kernel for those.
 template <class S, class C, int CM>
 __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel(const SweepArgs<S, C> P) {
-    static_assert(sizeof(S) == 2 && sizeof(C) == 4 && cm_fast(CM), "pair step: 16-bit storage, fused collision");
+    static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair step: 16-bit storage, float compute");
     const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     const uint32_t row = P.div_seg.div(gw);
@@ -126,7 +127,10 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel
     auto xs = [&](int d) { return raw_bits<S>(wv[d]); };
     auto xp = [&](int d) { return raw_bits_again<S>(wv[d]); };
     auto ys = [&](int d, F2 y) { *reinterpret_cast<unsigned*>(P.b[opp_of(d)] + c) = pack_bits<S>(y); };
-    bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
+    if constexpr (cm_fast(CM))
+        bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
+    else
+        bgk_collide_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.col, P.inv_scale);
 }
 
 // Odd (pull + push) step.

@@ -410,13 +410,15 @@ __device__ __forceinline__ void abp_row(const SweepArgs<S, C>& P, int j, int k, 
     auto ys = [&](int d, F2 y) {
         if (valid) *reinterpret_cast<unsigned*>((d < 18 ? P.b[d] : const_cast<S*>(P.a[18])) + c) = pack_bits<S>(y);
     };
-    bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
+    if constexpr (cm_fast(CM))
+        bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
+    else
+        bgk_collide_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.col, P.inv_scale);
 }
 
 template <class S, class C, int BC, int CM>
 __global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(const SweepArgs<S, C> P) {
     static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair sweep: 16-bit storage, float compute");
-    static_assert(cm_fast(CM), "the pair sweep takes the fused collision");
     typedef Faces<BC> F;
     const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;

@@ -100,7 +100,7 @@ def main(argv=None) -> int:
                             lat = make(kind, pattern, case, l, m, n, fast=(mode == "fast"))
                             if lat.L.bgk_lattice_uses_tma(lat.h):
                                 path = "tma"
-                            elif pair == "on" and BYTES[kind] == 2 and case != "inflow" and mode == "fast":
+                            elif pair == "on" and BYTES[kind] == 2 and case != "inflow":
                                 path = "two-node" if pattern == "ab" else "two-node even step"
                             else:
                                 path = "one-node"

@@ -168,16 +168,17 @@ const char* bgk_last_error(void);
 const char* bgk_version(void);
 
 /* Two-node sweeps for the 16-bit kinds (FP16 / BF16 storage, FP32 compute)
-   with the fused-multiply-add collision (fast = 1), without obstacle and
-   without fused moments: every thread advances two nodes and the two
-   collisions run as one on packed FP32 pairs (lane-wise the same roundings:
-   results are bit-identical to the one-node sweep).  Where every node pair
-   (i, i + 1), i odd, is one aligned 32-bit word (library-owned lattices of
-   even l) the pair is adjacent and each population moves as one word;
-   otherwise the thread takes nodes i and i + 32.  Used by bgk_sweep and
-   lattice steps.  On by default; 0 selects the one-node sweep.  Returns the
-   previous setting (not thread-safe against concurrent launches).  No
-   counterpart in the reference. */
+   without obstacle and without fused moments: every thread advances two
+   nodes and the two collisions run as one on packed FP32 pairs (lane-wise the
+   same roundings: results are bit-identical to the one-node sweep).  Where
+   every node pair (i, i + 1), i odd, is one aligned 32-bit word (library-owned
+   lattices of even l) the pair is adjacent and each population moves as one
+   word, in either collision mode (and the AA pattern's even step runs in
+   pairs); otherwise, with the fused collision (fast = 1), the thread takes
+   nodes i and i + 32.  Used by bgk_sweep and lattice steps.  On by default;
+   0 selects the one-node sweep.  Returns the previous setting (not
+   thread-safe against concurrent launches).  No counterpart in the
+   reference. */
 int bgk_set_pair_kernels(int enable);
 
 #ifdef __cplusplus

@@ -1,11 +1,11 @@
-"""The two-node sweep of the 16-bit kinds (sweep_ab2_kernel: nodes i and
-i + 32 per thread, packed FP32 collision; taken with the fused-multiply-add
-collision) against the one-node sweep: bit-identical states for FP16 and
-BF16 storage, every boundary case, force-free and forced collisions, on
-library-owned lattices (aligned rows) and on the reference layout with odd
-paddings (rows starting anywhere in a segment), with row lengths that leave
-partial 64-node segments; and the even step of the in-place AA pattern in
-pairs (aa_even_pair_kernel)."""
+"""The two-node sweeps of the 16-bit kinds against the one-node sweep:
+bit-identical states for FP16 and BF16 storage, every boundary case, both
+collision modes, force-free and forced collisions.  Library-owned lattices
+(aligned rows) take the adjacent-pair sweep (sweep_abp_kernel) and, for the
+in-place AA pattern, the pair even step (aa_even_pair_kernel); the reference
+layout with odd paddings (rows starting anywhere in a segment) takes nodes i
+and i + 32 per thread (sweep_ab2_kernel, fused collision); row lengths leave
+partial 64-node segments."""
 import zlib
 
 import numpy as np
@@ -61,10 +61,11 @@ def _reference_layout(kind, case, shape, fast, on, ipad, jpad, steps=3):
 
 @pytest.mark.parametrize("kind", [2, 3])
 @pytest.mark.parametrize("case", [c for c in CASES if c != "none"])
-def test_pair_equals_one_node_sweep_on_lattices(kind, case):
+@pytest.mark.parametrize("fast", [False, True])
+def test_pair_equals_one_node_sweep_on_lattices(kind, case, fast):
     for shape in SHAPES:
-        a = _lattice(kind, case, shape, True, True)
-        b = _lattice(kind, case, shape, True, False)
+        a = _lattice(kind, case, shape, fast, True)
+        b = _lattice(kind, case, shape, fast, False)
         bad = np.argwhere(a != b)
         assert len(bad) == 0, (kind, case, shape, len(bad), bad[:5].tolist())
 
@@ -82,12 +83,13 @@ def test_pair_equals_one_node_sweep_on_reference_layout(kind, case, ipad, jpad):
 
 @pytest.mark.parametrize("kind", [2, 3])
 @pytest.mark.parametrize("case", [c for c in CASES if c != "none"])
-def test_aa_even_pair_step_equals_one_node_step(kind, case):
+@pytest.mark.parametrize("fast", [False, True])
+def test_aa_even_pair_step_equals_one_node_step(kind, case, fast):
     """The in-place pattern: even steps through aa_even_pair_kernel, odd steps
     through aa_odd_kernel, against both through the one-node kernels."""
     for shape in SHAPES:
-        a = _lattice(kind, case, shape, True, True, steps=6, pattern="aa")
-        b = _lattice(kind, case, shape, True, False, steps=6, pattern="aa")
+        a = _lattice(kind, case, shape, fast, True, steps=6, pattern="aa")
+        b = _lattice(kind, case, shape, fast, False, steps=6, pattern="aa")
         bad = np.argwhere(a != b)
         assert len(bad) == 0, (kind, case, shape, len(bad), bad[:5].tolist())
 
