@@ -74,6 +74,10 @@ def bind(L) -> None:
     L.bgk_lattice_status.restype = c_int
     L.bgk_lattice_set_sphere.argtypes = [c_void_p, c_double, c_double, c_double, c_double]
     L.bgk_lattice_set_sphere.restype = c_int
+    L.bgk_lattice_set_zhalo.argtypes = [c_void_p, c_int]
+    L.bgk_lattice_set_zhalo.restype = c_int
+    L.bgk_lattice_plane.argtypes = [c_void_p, c_int, c_int, POINTER(c_void_p), POINTER(c_size_t)]
+    L.bgk_lattice_plane.restype = c_int
     L.bgk_set_retained_bytes.argtypes = [c_size_t]
     L.bgk_set_retained_bytes.restype = c_int
     L.bgk_trim_memory.argtypes = []

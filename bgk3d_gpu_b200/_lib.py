@@ -45,6 +45,7 @@ class SweepParams(Structure):
         ("imin", c_int), ("imax", c_int), ("jmin", c_int), ("jmax", c_int),
         ("kmin", c_int), ("kmax", c_int),
         ("fast", c_int),
+        ("zhalo", c_int),
     ]
 
 

@@ -85,6 +85,15 @@ int validate(const bgk_sweep_params* p) {
                 return set_error(BGK_ERR_ARG, "obstacle leading dimensions too small");
         }
     }
+    if (p->zhalo & ~3) return set_error(BGK_ERR_ARG, "zhalo %d: only bits 0 and 1", p->zhalo);
+    if (p->zhalo) {
+        // a slab face reads the neighbour's populations from the halo plane; the
+        // outflow plane and the obstacle mask would need the neighbour's too
+        if (p->bcase == BC_INFLOW)
+            return set_error(BGK_ERR_UNSUPPORTED, "z-slab faces (zhalo) are not supported for the inflow case");
+        if (p->obs && p->imin <= p->imax)
+            return set_error(BGK_ERR_UNSUPPORTED, "z-slab faces (zhalo) are not supported with an obstacle");
+    }
     return BGK_OK;
 }
 

@@ -90,6 +90,7 @@ SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* cons
     A.bcase = p->bcase;
     A.generic = !(p->cte1 == 1.0 && p->cte0 == 0.0 && p->fx == 0.0 && p->fy == 0.0 && p->fz == 0.0);
     A.fast = (p->fast != 0 && sizeof(C) == 4) ? 1 : 0;
+    A.zhalo = p->zhalo & 3;
     return A;
 }
 

@@ -77,7 +77,7 @@ int one_step(bgk_lattice* L, cudaStream_t st, double* mom = nullptr) {
         if (int e = aa_step(&L->p, L->a, odd, mom, st)) return e;
     } else {
         const bool has_obs = L->p.obs && L->p.imin <= L->p.imax;
-        if (!mom && L->tma_ok && g_tma_kernels && !has_obs) {
+        if (!mom && L->tma_ok && g_tma_kernels && !has_obs && !L->p.zhalo) {
             if (int e = tma_step(L, st)) return e;
         } else if (int e = sweep_launch_mom(&L->p, L->a, L->b, mom, st)) {
             return e;
@@ -302,7 +302,30 @@ int bgk_lattice_status(const bgk_lattice* L) {
 int bgk_lattice_uses_tma(const bgk_lattice* L) {
     if (!L) return 0;
     const bool has_obs = L->p.obs && L->p.imin <= L->p.imax;
-    return (L->tma_ok && g_tma_kernels && !has_obs) ? 1 : 0;
+    return (L->tma_ok && g_tma_kernels && !has_obs && !L->p.zhalo) ? 1 : 0;
+}
+
+int bgk_lattice_set_zhalo(bgk_lattice* L, int flags) {
+    if (!L) return set_error(BGK_ERR_ARG, "null lattice");
+    if (flags && L->desc.pattern != BGK_PATTERN_AB)
+        return set_error(BGK_ERR_UNSUPPORTED, "z-slab faces need the AB pattern");
+    bgk_sweep_params q = L->p;
+    q.zhalo = flags;
+    if (int e = validate(&q)) return e;
+    drop_graph(L);
+    L->p.zhalo = flags;
+    return BGK_OK;
+}
+
+int bgk_lattice_plane(const bgk_lattice* L, int pop, int k, void** ptr, size_t* bytes) {
+    if (!L || !ptr || !bytes) return set_error(BGK_ERR_ARG, "null argument");
+    if (L->desc.pattern != BGK_PATTERN_AB) return set_error(BGK_ERR_UNSUPPORTED, "planes of AB lattices only");
+    if (pop < 0 || pop > 18 || k < 0 || k > L->desc.n + 1)
+        return set_error(BGK_ERR_ARG, "plane %d of population %d out of range", k, pop);
+    const long long nxy = (long long)L->nx * L->ny;
+    *ptr = static_cast<char*>(L->a[pop]) + (nxy * k - L->origin) * (long long)L->es;
+    *bytes = (size_t)nxy * L->es;
+    return BGK_OK;
 }
 
 int bgk_set_tma_kernels(int enable) {

@@ -59,6 +59,7 @@ template <class S, class C> struct SweepArgs {
     int bcase;             // BC_* (used by the batched kernel, which dispatches per tile)
     int generic;           // 1 unless the force-free shifted collision applies
     int fast;              // 1: fused-multiply-add collision (float compute only)
+    int zhalo;             // bit 0 / bit 1: the face k = 1 / k = n reads the halo plane as stored
 };
 
 // Equilibrium population p (0..4 -> 01..05) of the inflow face
@@ -214,11 +215,13 @@ __device__ __forceinline__ bool gather_at(const SweepArgs<S, C>& P, int i, int j
     const IDX oxp = (F::PX && i == P.l) ? (IDX)(1 - P.l) : (IDX)1;
     const IDX oym = (F::PY && j == 1) ? (IDX)(P.m - 1) * nx : -nx;
     const IDX oyp = (F::PY && j == P.m) ? (IDX)(1 - P.m) * nx : nx;
-    const IDX ozm = (F::PZ && k == 1) ? (IDX)(P.n - 1) * nxy : -nxy;
-    const IDX ozp = (F::PZ && k == P.n) ? (IDX)(1 - P.n) * nxy : nxy;
+    // a z face of a slab (P.zhalo) reads the halo plane as stored: no wrap, no wall, no lid
+    const bool zlo = k == 1 && !(P.zhalo & 1), zhi = k == P.n && !(P.zhalo & 2);
+    const IDX ozm = (F::PZ && zlo) ? (IDX)(P.n - 1) * nxy : -nxy;
+    const IDX ozp = (F::PZ && zhi) ? (IDX)(1 - P.n) * nxy : nxy;
     const bool wxm = F::WX && i == 1, wxp = F::WX && i == P.l;
     const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
-    const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
+    const bool wzm = F::WZ && zlo, wzp = F::WZ && zhi;
 #pragma unroll
     for (int d = 0; d < 18; ++d) {
         const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
@@ -232,7 +235,7 @@ __device__ __forceinline__ bool gather_at(const SweepArgs<S, C>& P, int i, int j
         if (cz == 1) bounce |= wzm; else if (cz == -1) bounce |= wzp;
         const S* src = bounce ? P.a[opp_of(d)] : P.a[d];
         C v = Conv<S, C>::raw(ldro<S>(src + (bounce ? c : off)));
-        if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
+        if (BC == BC_DRIVEN && (d == 1 || d == 10) && zhi)
             v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force);
         if (BC == BC_INFLOW && cx == 1 && i == 1)
             v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
@@ -343,10 +346,11 @@ __device__ __forceinline__ void abp_row(const SweepArgs<S, C>& P, int j, int k, 
     const bool edge_lo = lane == 0 || at_lo, edge_hi = lane == 31 || at_hi;
     const int oym = (F::PY && j == 1) ? (P.m - 1) * nx : -nx;
     const int oyp = (F::PY && j == P.m) ? (1 - P.m) * nx : nx;
-    const int ozm = (F::PZ && k == 1) ? (P.n - 1) * nxy : -nxy;
-    const int ozp = (F::PZ && k == P.n) ? (1 - P.n) * nxy : nxy;
+    const bool zlo = k == 1 && !(P.zhalo & 1), zhi = k == P.n && !(P.zhalo & 2);   // slab faces: halo
+    const int ozm = (F::PZ && zlo) ? (P.n - 1) * nxy : -nxy;
+    const int ozp = (F::PZ && zhi) ? (1 - P.n) * nxy : nxy;
     const bool wym = WALLS && F::WY && j == 1, wyp = WALLS && F::WY && j == P.m;
-    const bool wzm = WALLS && F::WZ && k == 1, wzp = WALLS && F::WZ && k == P.n;
+    const bool wzm = WALLS && F::WZ && zlo, wzp = WALLS && F::WZ && zhi;
     // all loads first (no branch between them, so they are in flight
     // together): the pair word of every population and, for c_x != 0, the
     // one element the lane may need from outside its warp or across a face
@@ -392,7 +396,7 @@ __device__ __forceinline__ void abp_row(const SweepArgs<S, C>& P, int j, int k, 
             const uint32_t hi = edge_hi ? e[d] : right;
             if (!wall[d]) v = __byte_perm(v, hi, 0x5432);
         }
-        if (WALLS && BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n) {
+        if (WALLS && BC == BC_DRIVEN && (d == 1 || d == 10) && zhi) {
             // lid term, rounded to storage: the packed word holds it exactly
             F2 f = raw_bits<S>(v);
             f.v.x = roundtrip<S, C>(d == 1 ? f.v.x + P.lid_force : f.v.x - P.lid_force);
@@ -434,7 +438,8 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(co
     // the driven cavity's rows inside its walls run without wall logic
     // (measured +12 % at 256^3); for the channel the split costs registers
     // (spills) and runs slower, so every channel row takes the wall path
-    const bool wall_row = (F::WY && (j == 1 || j == P.m)) || (F::WZ && (k == 1 || k == P.n));
+    const bool wall_row = (F::WY && (j == 1 || j == P.m)) ||
+                          (F::WZ && ((k == 1 && !(P.zhalo & 1)) || (k == P.n && !(P.zhalo & 2))));
     if (BC != BC_DRIVEN || wall_row) abp_row<S, C, BC, CM, true>(P, j, k, lane, ia, valid);
     else abp_row<S, C, BC, CM, false>(P, j, k, lane, ia, valid);
 }

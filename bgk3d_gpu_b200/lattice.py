@@ -207,6 +207,19 @@ class Lattice:
         o = np.ascontiguousarray(obs, np.int32)
         check(self.L.bgk_lattice_set_obstacle(self.h, o.ctypes.data), "set_obstacle")
 
+    def set_zhalo(self, flags: int) -> None:
+        """z faces that read the halo planes as stored (bgk_lattice_set_zhalo):
+        bit 0 the face k = 1, bit 1 the face k = n (z-slab decomposition)."""
+        check(self.L.bgk_lattice_set_zhalo(self.h, int(flags)), "bgk_lattice_set_zhalo")
+
+    def plane(self, pop: int, k: int) -> torch.Tensor:
+        """Plane k of population pop of the current state as a device tensor
+        view (storage representation; bgk_lattice_plane).  Valid until the next step."""
+        ptr, nb = ctypes.c_void_p(), ctypes.c_size_t()
+        check(self.L.bgk_lattice_plane(self.h, int(pop), int(k), ctypes.byref(ptr), ctypes.byref(nb)),
+              "bgk_lattice_plane")
+        return _device_bytes(ptr.value, nb.value, self.device)
+
     def set_sphere(self, center, r2: float) -> None:
         """Solid sphere obstacle built on the device (bgk_lattice_set_sphere)."""
         check(self.L.bgk_lattice_set_sphere(self.h, float(center[0]), float(center[1]), float(center[2]),
@@ -348,6 +361,19 @@ class Batch:
     @property
     def nodes(self) -> int:
         return int(self.L.bgk_batch_nodes(self.h))
+
+
+class _DeviceRegion:
+    """__cuda_array_interface__ of nbytes bytes of device memory at ptr."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def _device_bytes(ptr: int, nbytes: int, device) -> torch.Tensor:
+    """A uint8 tensor viewing device memory the library owns (no copy)."""
+    return torch.as_tensor(_DeviceRegion(ptr, nbytes), device=device)
 
 
 def set_retained_bytes(nbytes: int) -> None:

@@ -79,11 +79,16 @@ typedef struct bgk_sweep_params {
                                  float compute (kinds F32, F16, BF16): fewer instructions,
                                  results within a few units in the last place per step.
                                  Ignored for double compute. */
+    int zhalo;                /* z faces that read the halo plane as stored (a slab of a
+                                 lattice split along z; the planes k = 0 / n+1 hold the
+                                 neighbour slab's populations): bit 0 the face k = 1, bit 1
+                                 the face k = n.  Such a face has no wrap, wall or lid.
+                                 0 (default): the case's own z rule at both faces. */
 } bgk_sweep_params;
 
 /* Fill *p with the reference's constants (p0 = 1/3, p1 = 1/18, p2 = 1/36,
    rf = tre = 3, qf = 1.5, cte1 = 1, cte0 = 0), no force, no obstacle,
-   bcase NONE, scale 1, nx = l+2, ny = m+2, fast 0. */
+   bcase NONE, scale 1, nx = l+2, ny = m+2, fast 0, zhalo 0. */
 void bgk_sweep_params_init(bgk_sweep_params* p, int kind, int l, int m, int n, double omega);
 
 /* One fused time step: boundary rules + pull-stream + BGK collision from the

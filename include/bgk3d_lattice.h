@@ -162,6 +162,22 @@ int bgk_lattice_uses_tma(const bgk_lattice* lat);
 int bgk_set_tma_kernels(int enable);
 int bgk_lattice_status(const bgk_lattice* lat);
 
+/* z-slab decomposition (a lattice split along z over several devices or
+   processes, one slab each).  bgk_lattice_set_zhalo(lat, flags): the faces
+   in flags (bit 0: k = 1, bit 1: k = n) read the populations that enter
+   through them from the halo planes k = 0 / n+1 as stored, with no wrap,
+   wall or lid there; the caller fills those planes from the neighbour slabs
+   before every step.  AB pattern only; not with the inflow case or an
+   obstacle (both would need the neighbour's outflow plane or mask).
+   bgk_lattice_plane(lat, pop, k, &ptr, &bytes): device address and size of
+   plane k (0..n+1) of population pop (0..18) of the current state, the
+   (nx * ny)-element region that holds its nodes (1..l, 1..m) contiguously:
+   what a halo exchange sends (planes 1 and n) and receives (planes 0 and
+   n+1).  Valid until the next step (the two population sets swap).  No
+   counterpart in the reference (which runs on one GPU). */
+int bgk_lattice_set_zhalo(bgk_lattice* lat, int flags);
+int bgk_lattice_plane(const bgk_lattice* lat, int pop, int k, void** ptr, size_t* bytes);
+
 /* Steps advanced since the last load. */
 long long bgk_lattice_steps(const bgk_lattice* lat);
 
