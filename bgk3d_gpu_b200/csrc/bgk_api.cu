@@ -52,7 +52,22 @@ long long sweep_blocks(const bgk_sweep_params* p, const void* a0) {
         aligned = (((elem & 31) + 1) % 32 == 0) && (p->nx % 32 == 0);
     }
     const long long nseg = aligned ? (p->l + 31) / 32 : (p->l + 62) / 32;
-    return (nseg * p->m * p->n + 7) / 8;
+    // the upper bound over alignments is the unaligned count
+    const long long nseg_max = (p->l + 62) / 32;
+    return mom_grid(((a0 ? nseg : nseg_max) * p->m * p->n + 7) / 8);
+}
+
+long long mom_grid(long long blocks) {
+    static int nsm[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& n = nsm[dev >= 0 && dev < 64 ? dev : 0];
+    if (n == 0) {
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 1;
+    }
+    const long long g = 20LL * n;
+    return blocks < g ? blocks : g;
 }
 
 int finalize_moments(const double* partials, long long nparts, double* out, cudaStream_t st) {

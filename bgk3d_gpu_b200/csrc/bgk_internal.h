@@ -31,8 +31,13 @@ int sweep_launch(const struct bgk_sweep_params* p, void* const* a, void* const* 
 // Same, with the per-block FP64 moments of the new state written to mom.
 int sweep_launch_mom(const struct bgk_sweep_params* p, void* const* a, void* const* b, double* mom,
                      cudaStream_t st);
-// Number of blocks (= partial-moment slots) of the sweep launch for p with
-// population 01 at a0 (nullptr: the upper bound for any alignment).
+// Blocks of a sweep launch that also produces moments: a fixed grid (20
+// blocks per SM of the current device, fewer for small lattices) strides over
+// the step's warps.  The partial sums, and so the last bits of the moments,
+// depend on the device's SM count, never on timing.
+long long mom_grid(long long blocks);
+// Number of blocks (= partial-moment slots) of the sweep launch with moments
+// for p with population 01 at a0 (nullptr: the upper bound for any alignment).
 long long sweep_blocks(const struct bgk_sweep_params* p, const void* a0);
 // Second pass over nparts partials of 5 doubles into out[0..4].
 int finalize_moments(const double* partials, long long nparts, double* out, cudaStream_t st);

@@ -103,6 +103,7 @@ void segment_geometry(SweepArgs<S, C>& A, const void* a0) {
     A.nseg_aligned = aligned ? 1 : 0;
     A.nseg = aligned ? (A.l + 31) / 32 : (A.l + 62) / 32;
     A.nrows = (uint32_t)((long long)A.m * A.n);
+    A.nwarps = (uint32_t)((long long)A.nseg * A.nrows);
     A.div_seg.init((uint32_t)A.nseg);
     A.div_m.init((uint32_t)A.m);
 }

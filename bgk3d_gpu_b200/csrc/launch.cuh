@@ -114,7 +114,7 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
     const int cm = coll_mode(A);
     const bool obs = A.obs != nullptr;
-    const unsigned nb = (unsigned)blocks;
+    const unsigned nb = (unsigned)(mom ? mom_grid(blocks) : blocks);
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
         if (g_pair_kernels && !obs && mom == nullptr && nelem < (1LL << 31) && pairs_aligned<S>(p, a, b)) {
             // adjacent node pairs: 64-node segments from i = 1
@@ -281,7 +281,7 @@ int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* m
     A.mom = mom;
     const long long warps = (long long)A.nseg * p->m * p->n;
     if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
-    const unsigned blocks = (unsigned)((warps + 7) / 8);
+    const unsigned blocks = (unsigned)(mom ? mom_grid((warps + 7) / 8) : (warps + 7) / 8);
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
         const int cm = coll_mode(A);

@@ -34,9 +34,8 @@ namespace bgk {
 // Node of this thread under the warp-segment mapping of sweep_ab_kernel;
 // returns false for idle lanes.
 template <class S, class C, class IDX>
-__device__ __forceinline__ bool aa_node(const SweepArgs<S, C>& P, int& i, int& j, int& k, IDX& c) {
+__device__ __forceinline__ bool aa_node(const SweepArgs<S, C>& P, uint32_t gw, int& i, int& j, int& k, IDX& c) {
     const int lane = threadIdx.x & 31;
-    const uint32_t gw = blockIdx.x * 8u + (threadIdx.x >> 5);
     const uint32_t row = P.div_seg.div(gw);
     if (row >= P.nrows) return false;
     const int seg = (int)(gw - row * (uint32_t)P.nseg);
@@ -54,10 +53,10 @@ __device__ __forceinline__ bool aa_node(const SweepArgs<S, C>& P, int& i, int& j
 // Even (local) step.  P.a and P.b both name the slot arrays.  Arithmetic in
 // storage units, as in sweep_node.
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
-__device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
+__device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
     int i, j, k;
     IDX c;
-    if (!aa_node<S, C, IDX>(P, i, j, k, c)) return;
+    if (!aa_node<S, C, IDX>(P, gw, i, j, k, c)) return;
     if (OBS && P.obs != nullptr && i >= P.imin && i <= P.imax && j >= P.jmin && j <= P.jmax &&
         k >= P.kmin && k <= P.kmax && (obstacle_links(P, i, j, k) & 0x80000000u))
         return;
@@ -94,8 +93,13 @@ __device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, double (&
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    aa_even_node<S, C, BC, IDX, CM, OBS>(P, m5);
-    if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
+    const uint32_t w0 = blockIdx.x * 8u + (threadIdx.x >> 5);
+    if (P.mom == nullptr) {
+        aa_even_node<S, C, BC, IDX, CM, OBS>(P, w0, m5);
+        return;
+    }
+    for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) aa_even_node<S, C, BC, IDX, CM, OBS>(P, gw, m5);
+    block_reduce_store<5>(m5, P.mom);
 }
 
 // Even step of the 16-bit kinds on aligned pairs
@@ -135,11 +139,11 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel
 
 // Odd (pull + push) step.
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
-__device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m5)[5]) {
+__device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
     typedef Faces<BC> F;
     int i, j, k;
     IDX c;
-    if (!aa_node<S, C, IDX>(P, i, j, k, c)) return;
+    if (!aa_node<S, C, IDX>(P, gw, i, j, k, c)) return;
     uint32_t sl = 0;
     if (OBS && P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
         j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1) {
@@ -243,8 +247,13 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, double (&m
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    aa_odd_node<S, C, BC, IDX, CM, OBS>(P, m5);
-    if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
+    const uint32_t w0 = blockIdx.x * 8u + (threadIdx.x >> 5);
+    if (P.mom == nullptr) {
+        aa_odd_node<S, C, BC, IDX, CM, OBS>(P, w0, m5);
+        return;
+    }
+    for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) aa_odd_node<S, C, BC, IDX, CM, OBS>(P, gw, m5);
+    block_reduce_store<5>(m5, P.mom);
 }
 
 // Outflow halo in slot form for a freshly loaded Layout E state: halo cell

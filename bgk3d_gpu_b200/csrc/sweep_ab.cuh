@@ -54,6 +54,7 @@ template <class S, class C> struct SweepArgs {
     int nseg;              // 32-node segments per row
     int nseg_aligned;      // 1 when every row starts on a segment boundary
     uint32_t nrows;        // m * n
+    uint32_t nwarps;       // nseg * nrows: the warps of one step
     FastDiv div_seg, div_m;
     double* mom;           // optional: per-block FP64 partial moments of the new state
     int bcase;             // BC_* (used by the batched kernel, which dispatches per tile)
@@ -254,14 +255,23 @@ __device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j,
     collide_store<S, C, IDX, CM>(P, x, (IDX)P.nx * (IDX)j + (IDX)P.nxy * (IDX)k + (IDX)i, m5);
 }
 
-// One launch = one time step.  With P.mom set, every block also writes the
+// One launch = one time step.  With P.mom set (a grid of mom_grid blocks
+// striding over the warps), every block also writes the
 // FP64 sums of SRC/diagno.F90's per-node moments of the state it produced
 // (fluid nodes) to P.mom[blockIdx.x * 5 ..].
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __global__ void __launch_bounds__(256, (SweepBlocks<S, C>::value)) sweep_ab_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    sweep_node<S, C, BC, IDX, CM, OBS>(P, blockIdx.x * 8u + (threadIdx.x >> 5), m5);
-    if (P.mom != nullptr) block_reduce_store<5>(m5, P.mom);
+    const uint32_t w0 = blockIdx.x * 8u + (threadIdx.x >> 5);
+    if (P.mom == nullptr) {
+        sweep_node<S, C, BC, IDX, CM, OBS>(P, w0, m5);
+        return;
+    }
+    // with moments: a fixed grid strides over the step's warps, so each
+    // thread accumulates many nodes and the block reduction runs once per
+    // block (per 256 nodes it had cost as many instructions as the sums)
+    for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) sweep_node<S, C, BC, IDX, CM, OBS>(P, gw, m5);
+    block_reduce_store<5>(m5, P.mom);
 }
 
 // Two nodes per thread for the 16-bit kinds: a warp owns 64 consecutive
