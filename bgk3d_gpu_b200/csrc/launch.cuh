@@ -66,8 +66,8 @@ template <class S, class C, int BC, class IDX, int CM, bool OBS> struct Ab2Launc
 };
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbpLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
-        if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && !OBS && sizeof(IDX) == 4)
-            sweep_abp_kernel<S, C, BC, CM><<<blocks, kPairThreads, 0, st>>>(A);
+        if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && sizeof(IDX) == 4)
+            sweep_abp_kernel<S, C, BC, CM, OBS><<<blocks, kPairThreads, 0, st>>>(A);
     }
 };
 // True when every node pair (i, i + 1), i odd, is one aligned 32-bit word in
@@ -116,7 +116,7 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     const bool obs = A.obs != nullptr;
     const unsigned nb = (unsigned)(mom ? mom_grid(blocks) : blocks);
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
-        if (g_pair_kernels && !obs && mom == nullptr && nelem < (1LL << 31) && pairs_aligned<S>(p, a, b)) {
+        if (g_pair_kernels && mom == nullptr && nelem < (1LL << 31) && pairs_aligned<S>(p, a, b)) {
             // adjacent node pairs: 64-node segments from i = 1
             SweepArgs<S, C> A2 = A;
             A2.nseg = (p->l + 63) / 64;
@@ -125,11 +125,11 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
             constexpr int wpb = kPairThreads / 32;
             const unsigned nb2 = (unsigned)((w2 + wpb - 1) / wpb);
             switch (p->bcase) {
-                case BC_NONE: by_variant<AbpLaunch, S, C, BC_NONE>(nelem, cm, false, A2, nb2, st); break;
-                case BC_DRIVEN: by_variant<AbpLaunch, S, C, BC_DRIVEN>(nelem, cm, false, A2, nb2, st); break;
-                case BC_PERIODIC: by_variant<AbpLaunch, S, C, BC_PERIODIC>(nelem, cm, false, A2, nb2, st); break;
-                case BC_CHANNEL: by_variant<AbpLaunch, S, C, BC_CHANNEL>(nelem, cm, false, A2, nb2, st); break;
-                case BC_INFLOW: by_variant<AbpLaunch, S, C, BC_INFLOW>(nelem, cm, false, A2, nb2, st); break;
+                case BC_NONE: by_variant<AbpLaunch, S, C, BC_NONE>(nelem, cm, obs, A2, nb2, st); break;
+                case BC_DRIVEN: by_variant<AbpLaunch, S, C, BC_DRIVEN>(nelem, cm, obs, A2, nb2, st); break;
+                case BC_PERIODIC: by_variant<AbpLaunch, S, C, BC_PERIODIC>(nelem, cm, obs, A2, nb2, st); break;
+                case BC_CHANNEL: by_variant<AbpLaunch, S, C, BC_CHANNEL>(nelem, cm, obs, A2, nb2, st); break;
+                case BC_INFLOW: by_variant<AbpLaunch, S, C, BC_INFLOW>(nelem, cm, obs, A2, nb2, st); break;
             }
             return check_launch("sweep_abp_kernel");
         }

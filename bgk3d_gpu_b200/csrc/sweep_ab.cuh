@@ -340,7 +340,9 @@ __global__ void __launch_bounds__(256, 4) sweep_ab2_kernel(const SweepArgs<S, C>
 // halo.  A y/z wall bounces both nodes to their own opposite populations
 // (one aligned load).  The two collisions run as one on packed FP32 pairs
 // (bit-identical to the one-node sweep) and every store is one aligned
-// 32-bit word.  No obstacle, no fused moments, 32-bit element offsets.
+// 32-bit word.  Warps whose nodes touch an obstacle's box (grown by one
+// node) take the one-node rules node by node.  No fused moments, 32-bit
+// element offsets.
 constexpr int kPairThreads = 128;   // threads per block of sweep_abp_kernel
 constexpr int kPairBlocks = 7;      // resident blocks per SM it is compiled for (72 registers)
 
@@ -430,7 +432,7 @@ __device__ __forceinline__ void abp_row(const SweepArgs<S, C>& P, int j, int k, 
         bgk_collide_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.col, P.inv_scale);
 }
 
-template <class S, class C, int BC, int CM>
+template <class S, class C, int BC, int CM, bool OBS>
 __global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(const SweepArgs<S, C> P) {
     static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair sweep: 16-bit storage, float compute");
     typedef Faces<BC> F;
@@ -445,6 +447,17 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) sweep_abp_kernel(co
     const int i0 = seg * 64 + 2 * lane + 1;
     const bool valid = i0 < P.l;                      // l even: the pair (i0, i0 + 1) is inside
     const int ia = valid ? i0 : P.l - 1;              // other lanes read a valid pair, store nothing
+    if (OBS && P.obs != nullptr && j >= P.jmin - 1 && j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1 &&
+        seg * 64 + 64 >= P.imin - 1 && seg * 64 + 1 <= P.imax + 1) {
+        // the warp's 64 nodes touch the obstacle's box grown by one node:
+        // the one-node rules (solid nodes skipped, links into solids bounced)
+        double m5[5];
+        if (valid) {
+            sweep_at<S, C, BC, int, CM, true>(P, ia, j, k, m5);
+            sweep_at<S, C, BC, int, CM, true>(P, ia + 1, j, k, m5);
+        }
+        return;
+    }
     // the driven cavity's rows inside its walls run without wall logic
     // (measured +12 % at 256^3); for the channel the split costs registers
     // (spills) and runs slower, so every channel row takes the wall path

@@ -100,8 +100,10 @@ def main(argv=None) -> int:
                             lat = make(kind, pattern, case, l, m, n, fast=(mode == "fast"))
                             if lat.L.bgk_lattice_uses_tma(lat.h):
                                 path = "tma"
+                            elif pair == "on" and BYTES[kind] == 2 and pattern == "ab":
+                                path = "two-node"
                             elif pair == "on" and BYTES[kind] == 2 and case != "inflow":
-                                path = "two-node" if pattern == "ab" else "two-node even step"
+                                path = "two-node even step"
                             else:
                                 path = "one-node"
                             s = time_steps(lat, args.steps, args.warmup)

@@ -173,7 +173,8 @@ const char* bgk_last_error(void);
 const char* bgk_version(void);
 
 /* Two-node sweeps for the 16-bit kinds (FP16 / BF16 storage, FP32 compute)
-   without obstacle and without fused moments: every thread advances two
+   without fused moments (warps next to an obstacle advance their nodes one
+   by one): every thread advances two
    nodes and the two collisions run as one on packed FP32 pairs (lane-wise the
    same roundings: results are bit-identical to the one-node sweep).  Where
    every node pair (i, i + 1), i odd, is one aligned 32-bit word (library-owned

@@ -136,3 +136,35 @@ def test_device_sphere_touching_the_walls_is_refused_like_the_mask():
     with pytest.raises(BGKError):
         lat.set_obstacle(CS.obstacle_mask(case))
     lat.close()
+
+
+def test_memory_pool_retains_and_trims():
+    """Lattice memory comes from the library's pool: with a retention budget
+    a closed lattice's memory stays with the pool (and the next lattice of
+    that size reuses it without taking more from the device); trimming gives
+    it back; with the default retention of 0 it goes back at once."""
+    import torch
+    from bgk3d_gpu_b200.lattice import Lattice, set_retained_bytes, trim_memory
+    shape = (128, 128, 128)
+    torch.cuda.synchronize()
+    try:
+        set_retained_bytes(8 << 30)
+        free0, _ = torch.cuda.mem_get_info()
+        lat = Lattice(*shape, kind=1, bcase="periodic", omega=1.5)
+        nbytes = lat.device_bytes
+        lat.close()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free0 - free1 >= 0.9 * nbytes          # still held by the pool
+        lat = Lattice(*shape, kind=1, bcase="periodic", omega=1.5)
+        free2, _ = torch.cuda.mem_get_info()
+        assert abs(free2 - free1) < 0.1 * nbytes       # reused, nothing new mapped
+        lat.close()
+        trim_memory()
+        free3, _ = torch.cuda.mem_get_info()
+        assert free3 - free1 >= 0.9 * nbytes          # given back
+    finally:
+        set_retained_bytes(0)
+    lat = Lattice(*shape, kind=1, bcase="periodic", omega=1.5)
+    lat.close()
+    free4, _ = torch.cuda.mem_get_info()
+    assert abs(free4 - free3) < 0.1 * nbytes           # default: back at once

@@ -94,6 +94,35 @@ def test_aa_even_pair_step_equals_one_node_step(kind, case, fast):
         assert len(bad) == 0, (kind, case, shape, len(bad), bad[:5].tolist())
 
 
+@pytest.mark.parametrize("kind", [2, 3])
+@pytest.mark.parametrize("case", ["inflow", "periodic", "driven"])
+@pytest.mark.parametrize("fast", [False, True])
+def test_pair_with_obstacle_equals_one_node_sweep(kind, case, fast):
+    """Warps that touch the obstacle's box take the one-node rules inside the
+    pair sweep; the rest run in pairs."""
+    from bgk3d_gpu_b200 import cases as CS
+    from bgk3d_gpu_b200.lattice import Lattice
+    l, m, n = 140, 20, 18
+    p = CASE_PARAMS[case]
+    mask = CS.obstacle_mask(CS.sphere(l, m, n, kind="f32", diameter=7.0, center=(70.5, 10.0, 9.0)))
+    out = []
+    for on in (True, False):
+        prev = _switch(on)
+        try:
+            lat = Lattice(l, m, n, kind=kind, bcase=BCASE[case], omega=OMEGA, scale=SCALE[kind], fast=fast,
+                          lid_force=p.get("lid_force", 0.0), u_inflow=p.get("u_inflow", 0.0))
+            lat.set_obstacle(mask)
+            lat.upload(random_state(l, m, n, kind, seed=11, scale=SCALE[kind]))
+            lat.step(5)
+            out.append(interior(lat.download(), l, m, n))
+            lat.close()
+        finally:
+            _switch(bool(prev))
+    fluid = np.broadcast_to(mask == 0, out[0].shape)
+    bad = np.argwhere((out[0] != out[1]) & fluid)
+    assert len(bad) == 0, (kind, case, fast, len(bad), bad[:5].tolist())
+
+
 def test_pair_switch_default_on():
     prev = _switch(True)
     assert _switch(bool(prev)) == 1
