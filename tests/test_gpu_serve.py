@@ -34,17 +34,23 @@ def _alone(req):
     return st, m
 
 
-@pytest.mark.parametrize("mode,floor,fast", [("continuous", 8e6, False), ("continuous", 3e4, False),
-                                             ("shared", 0, False), ("continuous", 3e4, True)])
-def test_results_identical_alone_and_in_the_mix(mode, floor, fast):
+@pytest.mark.parametrize("mode,floor,fast,small", [("continuous", 8e6, False, "batch"),
+                                                   ("continuous", 3e4, False, "batch"),
+                                                   ("shared", 0, False, "batch"),
+                                                   ("continuous", 3e4, True, "batch"),
+                                                   ("continuous", 3e4, False, "streams"),
+                                                   ("shared", 0, True, "streams")])
+def test_results_identical_alone_and_in_the_mix(mode, floor, fast, small):
     """floor 3e4 nodes makes the shortest-work-first policy step only a few
     solves per round, so batches change membership between rounds.  With the
     fused collision the FP16 requests step alone through the two-node sweep
-    and in the mix through the batched one-node sweep: still bit-identical."""
+    and in the mix through the batched one-node sweep: still bit-identical.
+    With small="streams" the small solves step side by side on their own
+    streams instead of through the tile queue."""
     from bgk3d_gpu_b200.serve import Server
     trace = _trace(fast)
-    done, summary = Server(budget_bytes=20e9, max_chunk=25, floor_nodes=floor).run(trace, mode=mode,
-                                                                                 keep_states=True)
+    done, summary = Server(budget_bytes=20e9, max_chunk=25, floor_nodes=floor, small=small).run(
+        trace, mode=mode, keep_states=True)
     assert summary["requests"] == len(trace)
     assert summary["rounds"] > len(trace)       # solves shared rounds
     by_id = {d["rid"]: d for d in done}
