@@ -65,6 +65,11 @@ template <> struct Pack2<__nv_bfloat16> {
 // (lo = first element in memory).
 __device__ __forceinline__ uint32_t s_bits(__half v) { return __half_as_ushort(v); }
 __device__ __forceinline__ uint32_t s_bits(__nv_bfloat16 v) { return __bfloat16_as_ushort(v); }
+template <class S> __device__ __forceinline__ S bits_s(uint32_t b);
+template <> __device__ __forceinline__ __half bits_s<__half>(uint32_t b) { return __ushort_as_half((unsigned short)b); }
+template <> __device__ __forceinline__ __nv_bfloat16 bits_s<__nv_bfloat16>(uint32_t b) {
+    return __ushort_as_bfloat16((unsigned short)b);
+}
 template <class S> __device__ __forceinline__ F2 raw_bits(uint32_t w) {
     typename Pack2<S>::V v;
     memcpy(&v, &w, sizeof w);

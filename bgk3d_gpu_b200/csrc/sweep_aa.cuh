@@ -256,6 +256,146 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(con
     block_reduce_store<5>(m5, P.mom);
 }
 
+// Odd step of the 16-bit kinds on aligned pairs (the layout of
+// aa_even_pair_kernel; driven cavity, periodic and channel cases; no
+// obstacle, no fused moments).  Pull: population d of the pair's nodes comes
+// from slot opp(d) of the source row as one 32-bit word, the x-shifted half
+// through a lane shuffle as in sweep_abp_kernel (behind a wall: own slot d).
+// Push: population d of both nodes goes to slot d of the target row; for
+// c_x = +-1 the word at the lane's own pair position holds one value of this
+// lane and one of its neighbour lane (a shuffle), and the value that leaves
+// the warp (or crosses an x face: wrap, bounce-back into own slot opp(d))
+// is stored as a 16-bit value.  Every slot is written once, by the node that
+// read it (or, within a warp, after the neighbour lane's read through the
+// shuffled data), so the in-place update has no hazard.  Bit-identical to
+// aa_odd_kernel.
+template <class S, class C, int BC, int CM>
+__global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(const SweepArgs<S, C> P) {
+    static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair step: 16-bit storage, float compute");
+    static_assert(BC == BC_DRIVEN || BC == BC_PERIODIC || BC == BC_CHANNEL, "pair odd step: no inflow");
+    typedef Faces<BC> F;
+    const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const uint32_t row = P.div_seg.div(gw);
+    if (row >= P.nrows) return;                       // whole warp
+    const int seg = (int)(gw - row * (uint32_t)P.nseg);
+    const uint32_t kk = P.div_m.div(row);
+    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
+    const int k = (int)kk + 1;
+    const int i0 = seg * 64 + 2 * lane + 1;
+    const bool valid = i0 < P.l;                      // l even: the pair (i0, i0 + 1) is inside
+    const int ia = valid ? i0 : P.l - 1;              // other lanes read a valid pair, store nothing
+    const int nx = (int)P.nx, nxy = (int)P.nxy;
+    const int c = nx * j + nxy * k + ia;
+    const bool at_lo = ia == 1, at_hi = ia + 1 == P.l;
+    const bool edge_lo = lane == 0 || at_lo, edge_hi = lane == 31 || at_hi;
+    const int oym = (F::PY && j == 1) ? (P.m - 1) * nx : -nx;
+    const int oyp = (F::PY && j == P.m) ? (1 - P.m) * nx : nx;
+    const int ozm = (F::PZ && k == 1) ? (P.n - 1) * nxy : -nxy;
+    const int ozp = (F::PZ && k == P.n) ? (1 - P.n) * nxy : nxy;
+    const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
+    const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
+    // ---- pull (all loads first)
+    uint32_t w[18], e[18];
+    bool wall[18];
+#pragma unroll
+    for (int d = 0; d < 18; ++d) {
+        const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d);
+        bool wl = false;
+        int off = c;
+        if (cy == 1) { off += oym; wl |= wym; } else if (cy == -1) { off += oyp; wl |= wyp; }
+        if (cz == 1) { off += ozm; wl |= wzm; } else if (cz == -1) { off += ozp; wl |= wzp; }
+        wall[d] = wl;
+        const S* src = wl ? P.a[d] + c : P.a[opp_of(d)] + off;
+        w[d] = *reinterpret_cast<const unsigned*>(src);
+        if (cx == 1) {
+            const S* ep = (F::WX && at_lo) ? P.a[d] + c
+                                           : P.a[opp_of(d)] + off + ((F::PX && at_lo) ? P.l - 1 : -1);
+            e[d] = s_bits(*ep);
+        } else if (cx == -1) {
+            const S* ep = (F::WX && at_hi) ? P.a[d] + c + 1
+                                           : P.a[opp_of(d)] + off + ((F::PX && at_hi) ? 2 - P.l : 2);
+            e[d] = s_bits(*ep);
+        }
+    }
+    uint32_t wv[19];
+#pragma unroll
+    for (int d = 0; d < 18; ++d) {
+        const int cx = cx_of(d);
+        uint32_t v = w[d];
+        if (cx == 1) {
+            const uint32_t left = __shfl_up_sync(0xffffffffu, v, 1) >> 16;
+            const uint32_t lo = edge_lo ? e[d] : left;
+            if (!wall[d]) v = __byte_perm(lo, v, 0x5410);
+        } else if (cx == -1) {
+            const uint32_t right = __shfl_down_sync(0xffffffffu, v, 1) & 0xffffu;
+            const uint32_t hi = edge_hi ? e[d] : right;
+            if (!wall[d]) v = __byte_perm(v, hi, 0x5432);
+        }
+        if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n) {
+            F2 f = raw_bits<S>(v);
+            f.v.x = roundtrip<S, C>(d == 1 ? f.v.x + P.lid_force : f.v.x - P.lid_force);
+            f.v.y = roundtrip<S, C>(d == 1 ? f.v.y + P.lid_force : f.v.y - P.lid_force);
+            v = pack_bits<S>(f);
+        }
+        wv[d] = v;
+    }
+    wv[18] = *reinterpret_cast<const unsigned*>(P.a[18] + c);
+    // ---- collision, and the push of each population as soon as it is known
+    auto bounce_bits = [&](int od, uint32_t bits) -> uint32_t {   // lid on a wall-reflected value
+        if (BC == BC_DRIVEN && (od == 1 || od == 10) && k == P.n) {
+            const C r = Conv<S, C>::raw(bits_s<S>(bits));
+            return s_bits(Conv<S, C>::pack(od == 1 ? r + P.lid_force : r - P.lid_force));
+        }
+        return bits;
+    };
+    auto st16 = [&](int arr, int at, uint32_t bits) { *reinterpret_cast<unsigned short*>(P.b[arr] + at) = (unsigned short)bits; };
+    auto st32 = [&](int arr, int at, uint32_t word) { *reinterpret_cast<unsigned*>(P.b[arr] + at) = word; };
+    auto xs = [&](int d) { return raw_bits<S>(wv[d]); };
+    auto xp = [&](int d) { return raw_bits_again<S>(wv[d]); };
+    auto ys = [&](int d, F2 y) {
+        const uint32_t pk = pack_bits<S>(y);                  // lo: node ia, hi: node ia + 1
+        if (d == 18) {
+            if (valid) st32(18, c, pk);
+            return;
+        }
+        const int cx = cx_of(d), cy = cy_of(d), cz = cz_of(d), od = opp_of(d);
+        bool wl = false;
+        int off = c;                                          // target row: x + c_d in y and z
+        if (cy == 1) { off += oyp; wl |= wyp; } else if (cy == -1) { off += oym; wl |= wym; }
+        if (cz == 1) { off += ozp; wl |= wzp; } else if (cz == -1) { off += ozm; wl |= wzm; }
+        if (cx == 1) {
+            const uint32_t prev_b = __shfl_up_sync(0xffffffffu, pk, 1) >> 16;     // lane t-1's node ia+1
+            if (!valid) return;
+            if (wl) { st32(od, c, bounce_bits(od, pk & 0xffffu) | (bounce_bits(od, pk >> 16) << 16)); return; }
+            if (edge_lo) st16(d, off + 1, pk & 0xffffu);      // node ia -> ia + 1 (hi half only)
+            else st32(d, off, __byte_perm(prev_b, pk, 0x5410));
+            if (edge_hi) {                                    // node ia + 1 -> ia + 2 leaves the lane's word
+                if (at_hi && F::WX) st16(od, c + 1, bounce_bits(od, pk >> 16));
+                else st16(d, off + ((F::PX && at_hi) ? 2 - P.l : 2), pk >> 16);
+            }
+        } else if (cx == -1) {
+            const uint32_t next_a = __shfl_down_sync(0xffffffffu, pk, 1) & 0xffffu;  // lane t+1's node ia
+            if (!valid) return;
+            if (wl) { st32(od, c, bounce_bits(od, pk & 0xffffu) | (bounce_bits(od, pk >> 16) << 16)); return; }
+            if (edge_hi) st16(d, off, pk >> 16);              // node ia + 1 -> ia (lo half only)
+            else st32(d, off, __byte_perm(pk, next_a, 0x5432));
+            if (edge_lo) {                                    // node ia -> ia - 1 leaves the lane's word
+                if (at_lo && F::WX) st16(od, c, bounce_bits(od, pk & 0xffffu));
+                else st16(d, off + ((F::PX && at_lo) ? P.l - 1 : -1), pk & 0xffffu);
+            }
+        } else {
+            if (!valid) return;
+            if (wl) st32(od, c, bounce_bits(od, pk & 0xffffu) | (bounce_bits(od, pk >> 16) << 16));
+            else st32(d, off, pk);
+        }
+    };
+    if constexpr (cm_fast(CM))
+        bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
+    else
+        bgk_collide_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.col, P.inv_scale);
+}
+
 // Outflow halo in slot form for a freshly loaded Layout E state: halo cell
 // (l+1, j, k) slot opp(p), p = 10..14, from the populations of (l, j, k).
 template <class S, class C>
