@@ -354,7 +354,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (Taylor-Green vortex initial condition, BASELINE form)",
+        "data": "synthetic (Taylor-Green vortex initial condition, x = 2 pi (i-1)/l form)",
         "config": {"workload": WORKLOAD, "l": L_, "m": M_, "n": N_, "tau": TAU, "u0": U0,
                    "pattern": f"{args.pattern.upper()} (library-owned padded lattice, boundaries fused, CUDA graph)",
                    "l2": "inputs 2.6 GB > 126 MB L2 (no flush needed)",

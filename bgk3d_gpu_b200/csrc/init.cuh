@@ -2,7 +2,7 @@
 // written straight into a lattice (no host round trip), the device form of
 // SRC/init.F90:113-201.
 //
-// Flows (the BASELINE forms of the reference's cases):
+// Flows (the benchmark forms of the reference's cases: grid points at 2 pi (i-1)/l, ...):
 //   INIT_UNIFORM  rho = p[0], u = (p[1], p[2], p[3])   (rest: 1, 0, 0, 0)
 //   INIT_TGV      Taylor-Green: x = 2 pi (i-1)/l, ...,
 //                 u = u0 sin x cos y cos z, v = -u0 cos x sin y cos z, w = 0,
