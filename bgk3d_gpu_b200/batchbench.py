@@ -5,15 +5,16 @@ tau uniform in [0.52, 0.8]; half Kida vortex (periodic, u0 = 0.05), half
 Poiseuille channel (x, y periodic, z walls, body force g = 1e-6 as g/10 per
 population with c_x != 0, times rho); FP32; `steps` steps each.
 
-Three ways to run the same solves are timed (CUDA events, same stream):
+Four ways to run the same solves are timed (CUDA events):
   batched     one persistent tile-queue launch per step for all lattices,
               16-step CUDA graphs, tile shape / grid chosen by the autotuner;
   sequential  one lattice after another, each with its own launches replayed
               through that lattice's CUDA graph;
+  streams     the lattices' graphs on 8 side streams, side by side;
   plain       one lattice after another, one API call (= one launch) per step.
-All three give bit-identical final states (checked on every lattice).
+All give bit-identical final states (checked on every lattice).
 
-  python -m bgk3d_gpu_b200.batchbench [--count 96] [--steps 2000] [--seed 20261203]
+  python -m bgk3d_gpu_b200.batchbench [--count 96] [--steps 2000] [--seed 20261203] [--sides 32,48,...]
 """
 from __future__ import annotations
 
@@ -31,9 +32,9 @@ from .lattice import Batch
 SIDES = (32, 48, 64, 96, 128, 160)
 
 
-def make_specs(count: int, seed: int):
+def make_specs(count: int, seed: int, side_set=SIDES):
     rng = np.random.default_rng(seed)
-    sides = rng.choice(SIDES, size=count)
+    sides = rng.choice(side_set, size=count)
     taus = rng.uniform(0.52, 0.8, size=count)
     specs = []
     for i in range(count):
@@ -67,11 +68,11 @@ def timed(fn):
 
 
 def run(count: int = 96, steps: int = 2000, seed: int = 20261203, modes=("batched", "sequential", "plain"),
-        tune_steps: int = 4):
-    specs = make_specs(count, seed)
+        tune_steps: int = 4, side_set=SIDES):
+    specs = make_specs(count, seed, side_set)
     lats, states = build(specs)
     nodes = sum(c["l"] * c["m"] * c["n"] for c in specs)
-    out = {"workload": f"{count} lattices, sides {SIDES} seed {seed}, half Kida / half Poiseuille, FP32",
+    out = {"workload": f"{count} lattices, sides {tuple(side_set)} seed {seed}, half Kida / half Poiseuille, FP32",
            "lattices": count, "steps": steps, "nodes": nodes,
            "device_gb": round(sum(lat.device_bytes for lat in lats) / 1e9, 2)}
     finals = None
@@ -86,10 +87,11 @@ def run(count: int = 96, steps: int = 2000, seed: int = 20261203, modes=("batche
         finals = [lat.download() for lat in lats]
         batch.close()
         out["batched"] = {"seconds": t, "solves_per_s": count / t, "glups": nodes * steps / t / 1e9}
-    if "sequential" in modes:
+    if "sequential" in modes or "streams" in modes:
         reload(lats, states)
-        for lat in lats[:2]:
-            lat.step(32)                 # capture graphs outside the timed region
+        for lat in lats:
+            lat.step(32)                 # capture every lattice's graph outside the timed regions
+    if "sequential" in modes:
         reload(lats, states)
 
         def seq():
@@ -99,6 +101,24 @@ def run(count: int = 96, steps: int = 2000, seed: int = 20261203, modes=("batche
         out["sequential"] = {"seconds": t, "solves_per_s": count / t, "glups": nodes * steps / t / 1e9}
         if finals is not None:
             out["sequential"]["identical_to_batched"] = all(
+                np.array_equal(f, lat.download()) for f, lat in zip(finals, lats))
+    if "streams" in modes:
+        reload(lats, states)
+        side = [torch.cuda.Stream() for _ in range(8)]
+
+        def streams():
+            main = torch.cuda.current_stream()
+            for s in side:
+                s.wait_stream(main)
+            for i, lat in enumerate(lats):
+                with torch.cuda.stream(side[i % len(side)]):
+                    lat.step(steps)
+            for s in side:
+                main.wait_stream(s)
+        t = timed(streams)
+        out["streams"] = {"seconds": t, "solves_per_s": count / t, "glups": nodes * steps / t / 1e9}
+        if finals is not None:
+            out["streams"]["identical_to_batched"] = all(
                 np.array_equal(f, lat.download()) for f, lat in zip(finals, lats))
     if "plain" in modes:
         reload(lats, states)
@@ -113,7 +133,7 @@ def run(count: int = 96, steps: int = 2000, seed: int = 20261203, modes=("batche
             out["plain"]["identical_to_batched"] = all(
                 np.array_equal(f, lat.download()) for f, lat in zip(finals, lats))
     if "batched" in out:
-        for k in ("sequential", "plain"):
+        for k in ("sequential", "streams", "plain"):
             if k in out:
                 out[f"batched_vs_{k}"] = out["batched"]["solves_per_s"] / out[k]["solves_per_s"]
     for lat in lats:
@@ -126,9 +146,11 @@ def main(argv=None):
     ap.add_argument("--count", type=int, default=96)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=20261203)
-    ap.add_argument("--modes", default="batched,sequential,plain")
+    ap.add_argument("--modes", default="batched,sequential,streams,plain")
+    ap.add_argument("--sides", default=",".join(str(v) for v in SIDES), help="cube sides drawn from")
     args = ap.parse_args(argv)
-    res = run(args.count, args.steps, args.seed, tuple(args.modes.split(",")))
+    res = run(args.count, args.steps, args.seed, tuple(args.modes.split(",")),
+              side_set=tuple(int(v) for v in args.sides.split(",")))
     print(json.dumps(res), flush=True)
     return 0
 
