@@ -100,6 +100,8 @@ def lib() -> ctypes.CDLL:
     L.bgk_version.restype = c_char_p
     L.bgk_set_pair_kernels.argtypes = [c_int]
     L.bgk_set_pair_kernels.restype = c_int
+    L.bgk_abi_struct_size.argtypes = [c_int]
+    L.bgk_abi_struct_size.restype = c_size_t
     _bind_lattice(L)
     _lib = L
     return L

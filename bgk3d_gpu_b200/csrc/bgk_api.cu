@@ -6,6 +6,7 @@
 #include <cstring>
 #include <string>
 #include "bgk3d_b200.h"
+#include "bgk3d_lattice.h"
 #include "bgk_internal.h"
 #include "kernels.h"
 #include "reduce.cuh"
@@ -234,5 +235,13 @@ int bgk_dropin_finalize(const double* partials, long long nparts, double* out_de
 const char* bgk_last_error(void) { return g_last_error.c_str(); }
 
 const char* bgk_version(void) { return "bgk3d_b200 0.1 (sm_100a)"; }
+
+size_t bgk_abi_struct_size(int which) {
+    switch (which) {
+        case 0: return sizeof(bgk_sweep_params);
+        case 1: return sizeof(bgk_lattice_desc);
+        default: return 0;
+    }
+}
 
 }  // extern "C"

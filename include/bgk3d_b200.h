@@ -172,6 +172,12 @@ const char* bgk_last_error(void);
 /* Library version string. */
 const char* bgk_version(void);
 
+/* Size in bytes of the library's structs as compiled: 0 bgk_sweep_params,
+   1 bgk_lattice_desc (bgk3d_lattice.h); 0 for anything else.  A binding in
+   another language (Fortran bind(C) types, Python ctypes) checks its mirror
+   against it.  No counterpart in the reference. */
+size_t bgk_abi_struct_size(int which);
+
 /* Two-node sweeps for the 16-bit kinds (FP16 / BF16 storage, FP32 compute)
    without fused moments (warps next to an obstacle advance their nodes one
    by one): every thread advances two

@@ -78,3 +78,16 @@ def test_workspace_query(built):
     L = _lib.lib()
     assert L.bgk_reduce_workspace_bytes(256, 256, 256) >= 5 * 8
     assert L.bgk_version().decode().startswith("bgk3d_b200")
+
+
+def test_struct_mirrors_match_the_library():
+    """The ctypes mirrors of bgk_sweep_params and bgk_lattice_desc have the
+    size the library was compiled with (a field added on one side only
+    would shift every field after it).  A pure host call: no GPU needed."""
+    import ctypes
+    from bgk3d_gpu_b200._lib import SweepParams, lib
+    from bgk3d_gpu_b200._lattice_abi import LatticeDesc
+    L = lib()
+    assert L.bgk_abi_struct_size(0) == ctypes.sizeof(SweepParams)
+    assert L.bgk_abi_struct_size(1) == ctypes.sizeof(LatticeDesc)
+    assert L.bgk_abi_struct_size(7) == 0
