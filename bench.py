@@ -47,16 +47,11 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _traffic_from_profile():
-    """dram bytes per sweep launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "sweep_ab_f32_tgv256.md")
-    try:
-        for line in open(path):
-            if line.strip().startswith("dram_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].strip().split()[0]) * 1e6   # MB -> bytes
-    except OSError:
-        pass
-    return None
+def _config(ws: int) -> dict:
+    """The workload description, identical in both arms' JSON lines."""
+    return {"workload": WORKLOAD, "l": L_, "m": M_, "n": N_, "tau": TAU, "u0": U0,
+            "l2": "inputs larger than L2 (2 x 19 x 4 B x 258^3 = 2.6 GB of state > 126 MB), no flush",
+            "parallelism": f"replicas x{ws}"}
 
 
 class ClockSampler:
@@ -207,7 +202,7 @@ def run_reference_arm(args):
         "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (Taylor-Green vortex)",
-        "config": {"workload": WORKLOAD, "l": L_, "m": M_, "n": N_, "tau": TAU, "u0": U0},
+        "config": _config(args.gpus),
         "impl": "reference",
         "cpu_baseline": {"value": glups, "unit": "GLUPS", "cores": lat.nthreads, "kind": "port",
                          "sample": sample},
@@ -268,6 +263,7 @@ def fp16_side(steps: int = 500):
     for mode in ("fast", "strict"):
         lat = Lattice(L_, M_, N_, kind="f16", bcase="periodic", omega=OMEGA, scale=256.0, fast=(mode == "fast"))
         lat.init_flow("tgv", (U0,))
+        lat.prepare()
         lat.step(32)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -283,6 +279,91 @@ def fp16_side(steps: int = 500):
     return out
 
 
+def fp16_accuracy(steps: int = 2000):
+    """Relative L2 velocity error of FP16-shifted storage (both collision
+    modes) and of FP32 against the FP64 path (bit-identical to the oracle) on
+    this workload: the Taylor-Green vortex, 256^3, `steps` steps from the
+    same on-device initial state.  About 3 s on one B200."""
+    import torch
+    from bgk3d_gpu_b200.lattice import Lattice
+    from bgk3d_gpu_b200.accuracy import velocity_field
+
+    def run(kind, fast=False):
+        sc = 256.0 if kind == "f16" else 1.0
+        lat = Lattice(L_, M_, N_, kind=kind, bcase="periodic", omega=OMEGA, scale=sc, fast=fast)
+        lat.init_flow("tgv", (U0,))
+        lat.step(steps)
+        rho, u = velocity_field(lat, sc)
+        lat.close()
+        return torch.stack(u)
+
+    ref = run("f64")
+    norm = float(torch.linalg.vector_norm(ref))
+    out = {"steps": steps, "against": "FP64 path (bit-identical to the oracle), same initial state"}
+    for name, kind, fast in (("f16_fast", "f16", True), ("f16_strict", "f16", False), ("f32", "f32", False)):
+        u = run(kind, fast)
+        out[name] = float(torch.linalg.vector_norm(u - ref)) / norm
+        del u
+    del ref
+    torch.cuda.empty_cache()
+    return out
+
+
+def dropin_kernel(steps: int = 400, warmup: int = 10):
+    """The drop-in step (bcond_periodic_gpu + col_mc_gpu of libbgk3d_dropin_sp.so)
+    on the caller's own layout (19 + 18 separate arrays of 258^3 floats, as
+    the Fortran driver allocates them), timed with CUDA events on the default
+    stream the library launches on: without and with the per-step FP64
+    moments fused into the step."""
+    import torch
+    from bgk3d_gpu_b200 import _lib
+    D = _lib.load_dropin(False)
+    peak, _ = _peaks()
+    host = tgv_host_state(torch.float32)
+    a = [host[d].cuda() for d in range(19)]
+    b = [torch.empty_like(a[0]) for _ in range(18)]
+    nx, ny = L_ + 2, M_ + 2
+    mom = torch.empty(5, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.default_stream()
+    res = {}
+    for track in (False, True):
+        D.bgk_dropin_reset()
+        D.bgk_dropin_track_moments(1 if track else 0)
+
+        def step():
+            pa = (ctypes.c_void_p * 19)(*[t.data_ptr() for t in a])
+            D.bcond_periodic_gpu(pa, L_, M_, N_, nx, ny)
+            D.col_mc_gpu(*[t.data_ptr() for t in a], *[t.data_ptr() for t in b], L_, M_, N_, nx, ny,
+                         OMEGA, 0.0, 1.0, 1 / 3, 1 / 18, 1 / 36, 3.0, 1.5, 3.0, 0.0, 0.0, 0.0)
+            for d in range(18):
+                a[d], b[d] = b[d], a[d]
+            if track and D.bgk_dropin_moments(mom.data_ptr(), None) != 0:
+                raise RuntimeError("bgk_dropin_moments failed")
+
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                step()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                step()
+            e1.record(stream)
+            e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        g = L_ * M_ * N_ / (ms * 1e-3) / 1e9
+        res["with_moments" if track else "step"] = {
+            "value": g, "unit": "GLUPS", "ms_per_step": ms,
+            "frac_of_measured_hbm": g * B_ALG_F32 / peak, "steps": steps}
+    D.bgk_dropin_track_moments(0)
+    D.bgk_dropin_reset()
+    del a, b, host
+    torch.cuda.empty_cache()
+    res["layout"] = f"reference (0:l+1, 0:m+1, 0:n+1), nx = {L_ + 2}, one allocation per population"
+    res["kernel"] = "sweep_ab_kernel<float,float,PERIODIC,int,CM_STRICT,false> (plane mapping)"
+    return res
+
+
 def run_ours(args):
     import torch
     ws, rank, local = _dist()
@@ -296,40 +377,49 @@ def run_ours(args):
     lat = Lattice(L_, M_, N_, kind="f32", bcase="periodic", omega=OMEGA, pattern=args.pattern)
     lat.upload(host.numpy())
     stream = torch.cuda.current_stream()
-    # warm-up includes the capture of the 16-step CUDA graph (first run of >= 32 steps)
-    args.warmup = max(args.warmup, 32)
+    # capture the 16-step CUDA graph now (nothing runs), so that the warm-up
+    # count is the driver's own and no capture falls into a timed region
+    lat.prepare()
     lat.step(args.warmup)
     torch.cuda.synchronize()
     _barrier(ws)
+    # K steps per timed region, repeated until at least 200 steps were timed;
+    # the median region is reported (each region: barrier + synchronize on
+    # both sides, CUDA events on the launching stream, max over ranks)
+    repeats = max(1, -(-200 // args.steps))
     clk = ClockSampler(local)
     clk.start()
     time.sleep(0.3)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    _barrier(ws)
-    e0.record(stream)
-    lat.step(args.steps)
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    nodes = L_ * M_ * N_
     from bgk3d_gpu_b200.replicas import job_throughput
-    _, t_max, rate = job_throughput(float(nodes) * args.steps, ms * 1e-3)
-    ms_max = t_max * 1e3
-    value = rate / 1e9
-    launch_s = ms * 1e-3 / args.steps
+    nodes = L_ * M_ * N_
+    region_ms = []
+    for _ in range(repeats):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        _barrier(ws)
+        e0.record(stream)
+        lat.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        _, t_max, _ = job_throughput(float(nodes) * args.steps, e0.elapsed_time(e1) * 1e-3)
+        region_ms.append(t_max * 1e3)
+    clocks = clk.stop()
+    ms_max = statistics.median(region_ms)
+    value = nodes * ws * args.steps / (ms_max * 1e-3) / 1e9
+    launch_s = ms_max * 1e-3 / args.steps
     achieved = B_ALG_F32 * nodes / launch_s / 1e9
     peak, peak_src = _peaks()
-    if args.steps % 2:
+    if lat.steps % 2:
         lat.step(1)
     ke = lat.moments()
+    timing = {"regions": repeats, "steps_per_region": args.steps, "stat": "median over regions",
+              "region_ms": region_ms}
     if args.kernel_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "GLUPS", "steps": args.steps,
                               "ms_per_step": ms_max / args.steps, "config": {"l": L_, "m": M_, "n": N_},
-                              "achieved_gbs": achieved, "kernel_only": True}), flush=True)
+                              "achieved_gbs": achieved, "kernel_only": True, "timing": timing}), flush=True)
         if ws > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -339,6 +429,8 @@ def run_ours(args):
     del lat
     torch.cuda.empty_cache()
     fp16 = fp16_side()
+    acc = fp16_accuracy()
+    dropin = dropin_kernel()
     e2e = run_e2e(host, args)
     torch.cuda.empty_cache()
     ref_cuda = ref_cuda_glups() if rank == 0 else None
@@ -349,32 +441,33 @@ def run_ours(args):
     if rank != 0:
         return 0
     cpu = cpu_sample()
-    traffic = _traffic_from_profile()
     line = {
         "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (Taylor-Green vortex initial condition, x = 2 pi (i-1)/l form)",
-        "config": {"workload": WORKLOAD, "l": L_, "m": M_, "n": N_, "tau": TAU, "u0": U0,
-                   "pattern": f"{args.pattern.upper()} (library-owned padded lattice, boundaries fused, CUDA graph)",
-                   "l2": "inputs 2.6 GB > 126 MB L2 (no flush needed)",
-                   "parallelism": f"replicas x{ws}"},
+        "config": _config(ws),
+        "setup": {"pattern": f"{args.pattern.upper()} (library-owned padded lattice, boundaries fused, "
+                             "CUDA graph of 16 steps for runs of 32 or more)"},
+        "timing": timing,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
-                     "traffic": traffic, "traffic_unit": "bytes per launch (ncu, profiles/sweep_ab_f32_tgv256.md)",
+                     "traffic": None,
+                     "traffic_note": "no counter is read in this run: DRAM read + write per launch from ncu "
+                                     "are in profiles/sweep_ab_f32_tgv256.md",
                      "algorithmic_bytes_per_launch": B_ALG_F32 * nodes, "b_alg_per_lup": B_ALG_F32,
-                     "kernel": "sweep_ab_kernel<float,float,PERIODIC,int,false>" if args.pattern == "ab"
-                     else "aa_odd_kernel + aa_even_kernel <float,float,PERIODIC,int,false>"},
+                     "kernel": "sweep_ab_kernel<float,float,PERIODIC,int,CM_STRICT,false>" if args.pattern == "ab"
+                     else "aa_odd_kernel + aa_even_kernel <float,float,PERIODIC,int,CM_STRICT,false>"},
         "cpu_baseline": {"value": cpu[0], "unit": "GLUPS", "cores": cpu[1], "kind": "port",
                          "sample": cpu[2]},
         "e2e": e2e,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * repeats,
         "clocks": clocks,
+        "dropin_kernel": dropin,
         "ref_cuda_sm100a_glups": ref_cuda,
         "fp16_shifted": {**fp16, "vs_f32_value": fp16["fast"]["value"] / value,
                          "vs_f32_value_strict": fp16["strict"]["value"] / value,
-                         "l2_velocity_rel_error": "3.3e-4 fused / 3.2e-4 reference order after 2000 steps "
-                                                  "(accuracy.py, profiles/accuracy_tgv256.md)",
+                         "l2_velocity_rel_error": acc,
                          "kernel": "sweep_abp_kernel<__half,float,PERIODIC,CM>"},
         "mass_sum_final": float(ke[0]), "ke_mean_final": float(ke[4] / nodes),
     }
@@ -455,6 +548,8 @@ def main():
                     help="two-lattice (ab) or in-place (aa) streaming")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the sweep only (no e2e, CPU or reference-CUDA legs): for ncu captures")
+    ap.add_argument("--dropin-only", action="store_true",
+                    help="time only the drop-in step on the reference layout (col_mc_gpu): for ncu captures")
     args = ap.parse_args()
     if args.lattice:
         global L_, M_, N_
@@ -463,6 +558,12 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.dropin_only:
+        import torch
+        torch.cuda.set_device(_dist()[2])
+        print(json.dumps({"dropin_kernel": dropin_kernel(args.steps), "config": {"l": L_, "m": M_, "n": N_}}),
+              flush=True)
+        return 0
     return run_ours(args)
 
 

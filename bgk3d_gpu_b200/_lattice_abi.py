@@ -90,12 +90,16 @@ def bind(L) -> None:
     L.bgk_lattice_store.restype = c_int
     L.bgk_lattice_step.argtypes = [c_void_p, c_int, c_void_p]
     L.bgk_lattice_step.restype = c_int
+    L.bgk_lattice_prepare.argtypes = [c_void_p]
+    L.bgk_lattice_prepare.restype = c_int
     L.bgk_lattice_step_moments.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p]
     L.bgk_lattice_step_moments.restype = c_int
     L.bgk_lattice_set_omega.argtypes = [c_void_p, c_double]
     L.bgk_lattice_set_omega.restype = c_int
     L.bgk_lattice_moments.argtypes = [c_void_p, c_void_p, c_void_p]
     L.bgk_lattice_moments.restype = c_int
+    L.bgk_lattice_dissipation.argtypes = [c_void_p, c_double, c_void_p, c_void_p]
+    L.bgk_lattice_dissipation.restype = c_int
     L.bgk_lattice_draglift.argtypes = [c_void_p] + [c_int] * 6 + [c_void_p, c_void_p]
     L.bgk_lattice_draglift.restype = c_int
     L.bgk_lattice_steps.argtypes = [c_void_p]

@@ -74,6 +74,10 @@ def lib() -> ctypes.CDLL:
     L.bgk_reduce_workspace_bytes.restype = c_size_t
     L.bgk_moments.argtypes = [P, POINTER(c_void_p), c_void_p, c_void_p, c_size_t, c_void_p]
     L.bgk_moments.restype = c_int
+    L.bgk_dissipation_workspace_bytes.argtypes = [c_int, c_int, c_int]
+    L.bgk_dissipation_workspace_bytes.restype = c_size_t
+    L.bgk_dissipation.argtypes = [P, POINTER(c_void_p), c_double, c_void_p, c_void_p, c_size_t, c_void_p]
+    L.bgk_dissipation.restype = c_int
     L.bgk_moments_noalloc.argtypes = [P, POINTER(c_void_p), c_void_p, c_void_p]
     L.bgk_moments_noalloc.restype = c_int
     L.bgk_moments_noalloc_max_bytes.argtypes = []

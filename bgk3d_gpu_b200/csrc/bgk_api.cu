@@ -10,6 +10,7 @@
 #include "bgk_internal.h"
 #include "kernels.h"
 #include "reduce.cuh"
+#include "dissipation.cuh"
 
 namespace bgk {
 
@@ -43,19 +44,15 @@ void moments_grid(int l, int m, int n, dim3& grd, dim3& blk) {
     grd = dim3((l + blk.x - 1) / blk.x, (m + blk.y - 1) / blk.y, kb);
 }
 
-long long sweep_blocks(const bgk_sweep_params* p, const void* a0) {
-    // the warp-segment launch of sweep_ab_kernel / the AA kernels: rows that
-    // start on a 32-element boundary need ceil(l/32) segments, others one more
+long long sweep_blocks(const bgk_sweep_params* p, const void* a0, bool one_node_ab) {
+    // the warp-segment launch of sweep_ab_kernel / the AA kernels (seg_plan);
+    // without a0 the upper bound over start alignments: the unaligned row
+    // mapping, which the plane mapping only replaces where it needs fewer warps
     const size_t es = p->kind == 0 ? 8 : (p->kind == 2 || p->kind == 3) ? 2 : 4;
-    bool aligned = false;
-    if (a0) {
-        const long long elem = (long long)((uintptr_t)a0 / es);
-        aligned = (((elem & 31) + 1) % 32 == 0) && (p->nx % 32 == 0);
-    }
-    const long long nseg = aligned ? (p->l + 31) / 32 : (p->l + 62) / 32;
-    // the upper bound over alignments is the unaligned count
-    const long long nseg_max = (p->l + 62) / 32;
-    return mom_grid(((a0 ? nseg : nseg_max) * p->m * p->n + 7) / 8);
+    const long long align = a0 ? (long long)(((uintptr_t)a0 / es) & 31) : 0;
+    const long long warps = a0 ? seg_plan(p->l, p->m, p->n, p->nx, align, one_node_ab).warps
+                               : (long long)((p->l + 62) / 32) * p->m * p->n;
+    return mom_grid((warps + 7) / 8);
 }
 
 long long mom_grid(long long blocks) {
@@ -130,6 +127,18 @@ int bgk::sweep_launch_mom(const bgk_sweep_params* p, void* const* a, void* const
     KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, mom, st)));
 }
 
+int bgk::dissipation_launch(const bgk_sweep_params* p, void* const* a, double nu, double* out, double* ws,
+                            cudaStream_t st) {
+    KIND_DISPATCH(p->kind, (launch_dissipation<S, C>(p, a, nu, out, ws, st)));
+}
+
+size_t bgk::dissipation_workspace(int l, int m, int n) {
+    dim3 grd, blk;
+    moments_grid(l, m, n, grd, blk);
+    const dim3 eg = enstrophy_grid(l, m, n);
+    return ((size_t)grd.x * grd.y * grd.z * 5 + (size_t)eg.x * eg.y * eg.z * 2) * sizeof(double);
+}
+
 int bgk::draglift_launch(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
                          int ke, double* out, double* ws, size_t ws_bytes, cudaStream_t st) {
     KIND_DISPATCH(p->kind, (launch_draglift<S, C>(p, a, is, ie, js, je, ks, ke, out, ws, ws_bytes, st)));
@@ -199,6 +208,23 @@ int bgk_moments(const bgk_sweep_params* p, void* const* a, double* out_dev, void
         return set_error(BGK_ERR_ARG, "workspace too small: %zu < %zu", workspace_bytes,
                          bgk_reduce_workspace_bytes(p->l, p->m, p->n));
     return bgk::moments_launch(p, a, out_dev, (double*)workspace, (cudaStream_t)stream);
+}
+
+size_t bgk_dissipation_workspace_bytes(int l, int m, int n) {
+    if (l < 1 || m < 1 || n < 1) return 0;
+    return bgk::dissipation_workspace(l, m, n);
+}
+
+int bgk_dissipation(const bgk_sweep_params* p, void* const* a, double nu, double* out_dev, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+    if (int e = validate(p)) return e;
+    if (!a || !out_dev || !workspace) return set_error(BGK_ERR_ARG, "null pointer");
+    for (int d = 0; d < 19; ++d)
+        if (!a[d]) return set_error(BGK_ERR_ARG, "null population %d", d + 1);
+    const size_t need = bgk::dissipation_workspace(p->l, p->m, p->n);
+    if (workspace_bytes < need) return set_error(BGK_ERR_ARG, "workspace too small: %zu < %zu", workspace_bytes, need);
+    if (!(nu >= 0.0)) return set_error(BGK_ERR_ARG, "viscosity must be >= 0");
+    return bgk::dissipation_launch(p, a, nu, out_dev, (double*)workspace, (cudaStream_t)stream);
 }
 
 int bgk_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks, int ke,

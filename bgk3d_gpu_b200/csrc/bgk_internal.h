@@ -5,6 +5,28 @@
 #include "bgk3d_b200.h"
 
 namespace bgk {
+// Warps of one step of the warp-segment sweeps (see sweep_ab.cuh).  Rows
+// that start on a 32-element boundary (the library's padded layout) take
+// ceil(l/32) warps each; other rows one more, unless the plane mapping
+// (allowed for the one-node AB sweep only) needs fewer warps: it tiles each
+// z plane's rows 1..m as one range, ceil((nx (m - 1) + l + 31) / 32) warps
+// for any start alignment.
+struct SegPlan {
+    bool aligned, flat;
+    long long nseg;    // warps per row (row mapping)
+    long long wpp;     // warps per plane (plane mapping)
+    long long warps;   // warps of one step
+};
+inline SegPlan seg_plan(int l, int m, int n, long long nx, long long align_base, bool allow_flat) {
+    SegPlan s;
+    s.aligned = ((align_base + 1) % 32 == 0) && (nx % 32 == 0);
+    s.nseg = s.aligned ? (l + 31) / 32 : (l + 62) / 32;
+    s.wpp = (nx * (m - 1) + l + 62) / 32;
+    s.flat = allow_flat && !s.aligned && nx * m < (1LL << 31) && s.wpp < s.nseg * m;
+    s.warps = s.flat ? s.wpp * n : s.nseg * m * n;
+    return s;
+}
+
 // TMA-staged sweep switch for library-owned lattices (bgk_set_tma_kernels).
 // Off by default: bit-exact, 280 instead of 408 instructions per node for
 // FP16, but measured at half the one-node kernel's rate on 256^3 (B200).
@@ -37,8 +59,10 @@ int sweep_launch_mom(const struct bgk_sweep_params* p, void* const* a, void* con
 // depend on the device's SM count, never on timing.
 long long mom_grid(long long blocks);
 // Number of blocks (= partial-moment slots) of the sweep launch with moments
-// for p with population 01 at a0 (nullptr: the upper bound for any alignment).
-long long sweep_blocks(const struct bgk_sweep_params* p, const void* a0);
+// for p with population 01 at a0 (nullptr: the upper bound for any alignment);
+// one_node_ab: the launch is the one-node AB sweep (plane mapping allowed),
+// false for the AA steps.
+long long sweep_blocks(const struct bgk_sweep_params* p, const void* a0, bool one_node_ab = true);
 // Second pass over nparts partials of 5 doubles into out[0..4].
 int finalize_moments(const double* partials, long long nparts, double* out, cudaStream_t st);
 // Device memory of library-owned objects from the per-device pool
@@ -48,6 +72,12 @@ int dev_alloc(void** p, size_t bytes, bool zero, const char* what);
 void dev_free(void* p);
 // Private non-blocking stream for set-up kernels and copies.
 cudaStream_t setup_stream();
+// The launches of the turbulence diagnostics (TKE, dissipation, mean
+// squares, enstrophy) into out[0..6], partials in ws.
+int dissipation_launch(const struct bgk_sweep_params* p, void* const* a, double nu, double* out, double* ws,
+                       cudaStream_t st);
+// Bytes of partial sums of dissipation_launch.
+size_t dissipation_workspace(int l, int m, int n);
 // The two launches of the FP64 drag/lift reduction.
 int draglift_launch(const struct bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks,
                     int ke, double* out, double* ws, size_t ws_bytes, cudaStream_t st);

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdint>
 #include "bgk3d_b200.h"
+#include "bgk_internal.h"
 #include "sweep_ab.cuh"
 #include "reduce.cuh"
 
@@ -94,18 +95,24 @@ SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* cons
     return A;
 }
 
-// Warp-segment launch geometry of sweep_ab_kernel (see sweep_ab.cuh).
+// Warp-segment launch geometry of sweep_ab_kernel (see sweep_ab.cuh);
+// allow_flat: the launch is the one-node AB sweep, which also knows the
+// plane mapping.
 template <class S, class C>
-void segment_geometry(SweepArgs<S, C>& A, const void* a0) {
+void segment_geometry(SweepArgs<S, C>& A, const void* a0, bool allow_flat = false) {
     const long long elem = (long long)((uintptr_t)a0 / sizeof(S));
     A.align_base = elem & 31;
-    const bool aligned = ((A.align_base + 1) % 32 == 0) && (A.nx % 32 == 0);
-    A.nseg_aligned = aligned ? 1 : 0;
-    A.nseg = aligned ? (A.l + 31) / 32 : (A.l + 62) / 32;
+    const SegPlan s = seg_plan(A.l, A.m, A.n, A.nx, A.align_base, allow_flat);
+    A.nseg_aligned = s.aligned ? 1 : 0;
+    A.nseg = (int)s.nseg;
     A.nrows = (uint32_t)((long long)A.m * A.n);
-    A.nwarps = (uint32_t)((long long)A.nseg * A.nrows);
+    A.nwarps = (uint32_t)s.warps;
     A.div_seg.init((uint32_t)A.nseg);
     A.div_m.init((uint32_t)A.m);
+    A.flat = s.flat ? 1 : 0;
+    A.fwpp = (uint32_t)s.wpp;
+    A.div_fw.init(A.fwpp);
+    A.div_nx.init((uint32_t)(A.nx < (1LL << 31) ? A.nx : 1));
 }
 
 // True unless the collision can use the shifted, force-free specialisation.

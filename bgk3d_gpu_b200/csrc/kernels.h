@@ -28,10 +28,13 @@ template <class S, class C>
 int launch_batch(const void* desc, const uint32_t* tile_begin, int nlat, uint32_t ntiles, unsigned* counter,
                  int parity, int sub, int grid, cudaStream_t st);
 template <class S, class C>
+int launch_dissipation(const bgk_sweep_params* p, void* const* a, double nu, double* out, double* ws,
+                       cudaStream_t st);
+template <class S, class C>
 int launch_outflow(const bgk_sweep_params* p, void* const* a, cudaStream_t st);
 template <class S, class C>
 int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n, int flow, const double* prm,
-                float scale, cudaStream_t st);
+                float scale, const bgk_sweep_params* p, cudaStream_t st);
 }  // namespace bgk
 
 // storage kinds: 0 f64/f64, 1 f32/f32, 2 f16/f32, 3 bf16/f32, 4 f32/f64

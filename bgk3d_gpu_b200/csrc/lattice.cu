@@ -117,7 +117,8 @@ int build_graph(bgk_lattice* L) {
 
 int ensure_workspace(const bgk_lattice* Lc) {
     bgk_lattice* L = const_cast<bgk_lattice*>(Lc);
-    const size_t need = std::max<size_t>(bgk_reduce_workspace_bytes(L->desc.l, L->desc.m, L->desc.n), 1 << 16);
+    const size_t need = std::max<size_t>({bgk_reduce_workspace_bytes(L->desc.l, L->desc.m, L->desc.n),
+                                          dissipation_workspace(L->desc.l, L->desc.m, L->desc.n), size_t(1) << 16});
     if (L->ws && L->ws_bytes >= need) return BGK_OK;
     dev_free(L->ws);
     L->ws = nullptr;
@@ -438,7 +439,7 @@ int bgk_lattice_load(bgk_lattice* L, const void* host, void* stream) {
 
 int bgk_lattice_init(bgk_lattice* L, int flow, const double* params, void* stream) {
     if (!L) return set_error(BGK_ERR_ARG, "null lattice");
-    if (flow < 0 || flow > 2) return set_error(BGK_ERR_ARG, "unknown flow %d", flow);
+    if (flow < 0 || flow > 4) return set_error(BGK_ERR_ARG, "unknown flow %d", flow);
     cudaStream_t st = (cudaStream_t)stream;
     void* f[19];
     bgk_lat::begin_load(L, f);
@@ -447,11 +448,11 @@ int bgk_lattice_init(bgk_lattice* L, int flow, const double* params, void* strea
     {
         const bgk_sweep_params* p = &L->p;
         switch (L->desc.kind) {
-            case K_F64: rc = launch_init<double, double>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
-            case K_F32: rc = launch_init<float, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
-            case K_F16: rc = launch_init<__half, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
-            case K_BF16: rc = launch_init<__nv_bfloat16, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
-            default: rc = launch_init<float, double>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, st); break;
+            case K_F64: rc = launch_init<double, double>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, p, st); break;
+            case K_F32: rc = launch_init<float, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, p, st); break;
+            case K_F16: rc = launch_init<__half, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, p, st); break;
+            case K_BF16: rc = launch_init<__nv_bfloat16, float>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, p, st); break;
+            default: rc = launch_init<float, double>(f, L->nx, L->ny, p->l, p->m, p->n, flow, params, scale, p, st); break;
         }
     }
     if (rc) return rc;
@@ -473,6 +474,24 @@ int bgk_lattice_store(const bgk_lattice* L, void* host, void* stream) {
         if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "store: %s", cudaGetErrorString(e));
     }
     return BGK_OK;
+}
+
+int bgk_lattice_prepare(bgk_lattice* L) {
+    if (!L) return set_error(BGK_ERR_ARG, "bad argument");
+    if (L->graph) return BGK_OK;
+    // the graph starts from the arrangement of an even step count
+    const long long saved = L->steps;
+    void* a0[19]; void* b0[19];
+    std::memcpy(a0, L->a, sizeof a0); std::memcpy(b0, L->b, sizeof b0);
+    if (L->steps % 2) {
+        if (L->desc.pattern == BGK_PATTERN_AB)
+            for (int d = 0; d < 18; ++d) std::swap(L->a[d], L->b[d]);
+        L->steps -= 1;
+    }
+    const int rc = build_graph(L);
+    L->steps = saved;
+    std::memcpy(L->a, a0, sizeof a0); std::memcpy(L->b, b0, sizeof b0);
+    return rc;
 }
 
 int bgk_lattice_step(bgk_lattice* L, int nsteps, void* stream) {
@@ -501,7 +520,7 @@ int bgk_lattice_step(bgk_lattice* L, int nsteps, void* stream) {
 int bgk_lattice_step_moments(bgk_lattice* L, int nsteps, int every, double* out_dev, void* stream) {
     if (!L || nsteps < 0 || every < 1 || !out_dev) return set_error(BGK_ERR_ARG, "bad argument");
     cudaStream_t st = (cudaStream_t)stream;
-    const long long nb = sweep_blocks(&L->p, L->a[0]);
+    const long long nb = sweep_blocks(&L->p, L->a[0], L->desc.pattern == BGK_PATTERN_AB);
     const size_t need = (size_t)nb * 5 * sizeof(double);
     if (L->mom_bytes < need) {
         dev_free(L->mom);
@@ -525,6 +544,17 @@ int bgk_lattice_set_omega(bgk_lattice* L, double omega) {
     L->p.omega = omega;
     L->desc.omega = omega;
     return BGK_OK;
+}
+
+int bgk_lattice_dissipation(const bgk_lattice* L, double nu, double* out_dev, void* stream) {
+    if (!L || !out_dev) return set_error(BGK_ERR_ARG, "null argument");
+    if (!(nu >= 0.0)) return set_error(BGK_ERR_ARG, "viscosity must be >= 0");
+    if (L->desc.pattern == BGK_PATTERN_AA && (L->steps % 2) != 0)
+        return set_error(BGK_ERR_STATE, "AA lattice after an odd number of steps holds no observable state");
+    if (int e = ensure_workspace(L)) return e;
+    void* obsv[19];
+    observable(L, obsv);
+    return dissipation_launch(&L->p, obsv, nu, out_dev, L->ws, (cudaStream_t)stream);
 }
 
 int bgk_lattice_moments(const bgk_lattice* L, double* out_dev, void* stream) {

@@ -12,6 +12,7 @@
 #include "reduce.cuh"
 #include "batch.cuh"
 #include "init.cuh"
+#include "dissipation.cuh"
 
 namespace bgk {
 
@@ -101,14 +102,14 @@ template <class S, class C> int coll_mode(const SweepArgs<S, C>& A) {
 template <class S, class C>
 int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st) {
     SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
-    segment_geometry(A, a[0]);
+    segment_geometry(A, a[0], true);
     A.mom = mom;
     if (p->bcase == BC_INFLOW) {
         dim3 blk(128), grd((p->m + 127) / 128, p->n);
         outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
         if (int e = check_launch("outflow_halo_kernel")) return e;
     }
-    const long long warps = (long long)A.nseg * p->m * p->n;
+    const long long warps = seg_plan(p->l, p->m, p->n, p->nx, A.align_base, true).warps;
     const long long blocks = (warps + 7) / 8;
     if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
@@ -248,6 +249,55 @@ int launch_moments(const bgk_sweep_params* p, void* const* a, double* out, doubl
     const long long nparts = (long long)grd.x * grd.y * grd.z;
     finalize_partials_kernel<5><<<1, kFinalizeThreads, 0, st>>>(ws, nparts, out);
     return check_launch("finalize_partials_kernel");
+}
+
+template <class S, class C, int BC>
+int launch_dissipation_bc(const bgk_sweep_params* p, const SweepArgs<S, C>& A, const FieldArgs<S, C>& F, C two_nu,
+                          double* out, double* ws, cudaStream_t st) {
+    dim3 grd, blk;
+    moments_grid(p->l, p->m, p->n, grd, blk);
+    const long long nb1 = (long long)grd.x * grd.y * grd.z;
+    const ColConst<C> K = col_const<C>(p, 1.0);
+    const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
+    if (nelem >= (1LL << 31))
+        dissipation_partial_kernel<S, C, BC, long long><<<grd, blk, 0, st>>>(A, K, two_nu, ws);
+    else
+        dissipation_partial_kernel<S, C, BC, int><<<grd, blk, 0, st>>>(A, K, two_nu, ws);
+    if (int e = check_launch("dissipation_partial_kernel")) return e;
+    finalize_partials_kernel<5><<<1, kFinalizeThreads, 0, st>>>(ws, nb1, out);
+    if (int e = check_launch("finalize_partials_kernel")) return e;
+    const dim3 eg = enstrophy_grid(p->l, p->m, p->n);
+    const long long nb2 = (long long)eg.x * eg.y * eg.z;
+    double* ws2 = ws + 5 * nb1;
+    enstrophy_partial_kernel<S, C, BC><<<eg, dim3(kEnsTX, kEnsTY), 0, st>>>(F, p->zhalo, ws2);
+    if (int e = check_launch("enstrophy_partial_kernel")) return e;
+    finalize_partials_kernel<2><<<1, kFinalizeThreads, 0, st>>>(ws2, nb2, out + 5);
+    return check_launch("finalize_partials_kernel");
+}
+
+// TKE, dissipation, mean squares and enstrophy (dissipation.cuh) into
+// out[0..6]; ws holds bgk_dissipation_workspace_bytes(l, m, n) bytes.  The
+// inflow case first writes the outflow halo plane of the current state, as
+// the reference's boundary routine does before its pull.
+template <class S, class C>
+int launch_dissipation(const bgk_sweep_params* p, void* const* a, double nu, double* out, double* ws,
+                       cudaStream_t st) {
+    SweepArgs<S, C> A = sweep_args<S, C>(p, a, a);
+    const FieldArgs<S, C> F = field_args<S, C>(p, a);
+    const C two_nu = C(2) * (C)nu;
+    switch (p->bcase) {
+        case BC_NONE: return launch_dissipation_bc<S, C, BC_NONE>(p, A, F, two_nu, out, ws, st);
+        case BC_DRIVEN: return launch_dissipation_bc<S, C, BC_DRIVEN>(p, A, F, two_nu, out, ws, st);
+        case BC_PERIODIC: return launch_dissipation_bc<S, C, BC_PERIODIC>(p, A, F, two_nu, out, ws, st);
+        case BC_CHANNEL: return launch_dissipation_bc<S, C, BC_CHANNEL>(p, A, F, two_nu, out, ws, st);
+        case BC_INFLOW: {
+            dim3 blk(128), grd((p->m + 127) / 128, p->n);
+            outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
+            if (int e = check_launch("outflow_halo_kernel")) return e;
+            return launch_dissipation_bc<S, C, BC_INFLOW>(p, A, F, two_nu, out, ws, st);
+        }
+    }
+    return set_error(BGK_ERR_ARG, "bcase %d", p->bcase);
 }
 
 template <class S, class C>
@@ -391,7 +441,21 @@ int launch_outflow(const bgk_sweep_params* p, void* const* a, cudaStream_t st) {
 
 template <class S, class C>
 int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n, int flow, const double* prm,
-                float scale, cudaStream_t st) {
+                float scale, const bgk_sweep_params* p, cudaStream_t st) {
+    if (flow == INIT_TGV_REF || flow == INIT_TG2D_REF) {
+        InitRefArgs<S, C> R;
+        for (int d = 0; d < 19; ++d) R.f[d] = (S*)f[d];
+        R.nx = nx; R.nxy = nx * ny;
+        R.l = l; R.m = m; R.n = n;
+        R.flow = flow;
+        R.u00 = (C)(prm ? prm[0] : 0.0);
+        R.rf = (C)p->rf; R.qf = (C)p->qf; R.tre = (C)p->tre;
+        R.p0 = (C)p->p0; R.p1 = (C)p->p1; R.p2 = (C)p->p2;
+        R.scale = scale;
+        const long long nodes = (long long)(l + 2) * (m + 2) * (n + 2);
+        init_reference_kernel<S, C><<<(unsigned)((nodes + 255) / 256), 256, 0, st>>>(R);
+        return check_launch("init_reference_kernel");
+    }
     InitArgs<S> A;
     for (int d = 0; d < 19; ++d) A.f[d] = (S*)f[d];
     A.nx = nx; A.nxy = nx * ny;
@@ -436,5 +500,7 @@ int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n,
     template int launch_aa_prepass<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);     \
     template int launch_outflow<S, C>(const bgk_sweep_params*, void* const*, cudaStream_t);        \
     template int launch_init<S, C>(void* const*, long long, long long, int, int, int, int,          \
-                                   const double*, float, cudaStream_t);                            \
+                                   const double*, float, const bgk_sweep_params*, cudaStream_t);   \
+    template int launch_dissipation<S, C>(const bgk_sweep_params*, void* const*, double, double*,  \
+                                          double*, cudaStream_t);                                  \
     }

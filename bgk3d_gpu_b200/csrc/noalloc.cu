@@ -15,7 +15,13 @@
 // host code is only a host-side stand-in, so the device address is obtained
 // with cudaGetSymbolAddress, once per device, with that device current, on
 // the first call made on that device (make that first call before any stream
-// capture).  All calls share the array and it keeps the previous call's
+// capture).  The address is kept for the life of the process: do not call
+// this entry point on a device after cudaDeviceReset of that device (the
+// module may then be loaded again elsewhere and the kept address would be
+// stale).  The 2 MiB hold the 40-byte partial sums of 52428 blocks of the
+// moments pass, ceil(l/tx) x ceil(m/ty) x min(n, 64) blocks with tx x ty =
+// 256 threads, tx the smallest power of two >= l in 32..256: 256^3 needs
+// 16384 blocks and is served, 512^3 needs 65536 and is rejected.  All calls share the array and it keeps the previous call's
 // contents: each launch overwrites every partial-sum slot it later reads, so
 // nothing has to start at zero, but calls that overlap on the GPU (different
 // streams, or different host threads, on the same device) race on it.

@@ -54,8 +54,13 @@ template <class S, class C> struct SweepArgs {
     int nseg;              // 32-node segments per row
     int nseg_aligned;      // 1 when every row starts on a segment boundary
     uint32_t nrows;        // m * n
-    uint32_t nwarps;       // nseg * nrows: the warps of one step
+    uint32_t nwarps;       // the warps of one step: nseg * nrows, or fwpp * n when flat
     FastDiv div_seg, div_m;
+    // plane mapping of the one-node AB sweep for rows that start mid-segment
+    // (the reference's own nx = l + 2 layout): flat = 1 when in use
+    int flat;
+    uint32_t fwpp;         // warps per z plane
+    FastDiv div_fw, div_nx;
     double* mom;           // optional: per-block FP64 partial moments of the new state
     int bcase;             // BC_* (used by the batched kernel, which dispatches per tile)
     int generic;           // 1 unless the force-free shifted collision applies
@@ -178,8 +183,35 @@ __device__ __forceinline__ void collide_store(const SweepArgs<S, C>& P, const C 
     }
 }
 
+// Plane mapping (P.flat): a warp owns 32 consecutive, 32-element aligned
+// elements of the range that runs from node (1, 1, k) to node (l, m, k) of
+// one z plane, rows back to back.  Lanes that land on a halo column (i = 0 or
+// i > l) idle: 2 of every nx lanes on the reference's nx = l + 2 layout,
+// where whole rows would cost one extra warp per row (9 warps for 256 nodes).
+template <class S, class C, int BC, class IDX, int CM, bool OBS>
+__device__ __forceinline__ void sweep_node_flat(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t kk = P.div_fw.div(gw);
+    if (kk >= (uint32_t)P.n) return;
+    const int s = (int)(gw - kk * P.fwpp);
+    const int k = (int)kk + 1;
+    const IDX first = (IDX)P.nx + (IDX)P.nxy * (IDX)k + 1;   // element of node (1, 1, k)
+    const int sh = (int)((P.align_base + (long long)first) & 31);
+    const int r = s * 32 + lane - sh;                      // element offset from node (1, 1, k)
+    if (r < 0) return;
+    const uint32_t jj = P.div_nx.div((uint32_t)r);
+    const int i = r - (int)jj * (int)P.nx + 1;
+    const int j = (int)jj + 1;
+    if (i > P.l || j > P.m) return;
+    sweep_at<S, C, BC, IDX, CM, OBS>(P, i, j, k, m5);
+}
+
 template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
+    if (P.flat) {
+        sweep_node_flat<S, C, BC, IDX, CM, OBS>(P, gw, m5);
+        return;
+    }
     const int lane = threadIdx.x & 31;
     const uint32_t row = P.div_seg.div(gw);
     if (row >= P.nrows) return;

@@ -121,6 +121,18 @@ class DeviceLattice:
                                 ws.numel(), st), "bgk_moments")
         return self._out[:5].cpu().numpy().copy()
 
+    def dissipation(self, nu: float) -> np.ndarray:
+        """FP64 turbulence diagnostics (SRC/dissipation.F90 and the enstrophy):
+        sum 0.5|u|^2, sum 2 nu Pi:Pi, sum u_x^2, u_y^2, u_z^2, sum 0.5|w|^2 and
+        the number of nodes in that last sum (bgk_dissipation)."""
+        nb = lib().bgk_dissipation_workspace_bytes(self.l, self.m, self.n)
+        ws = torch.empty(max(nb, 1 << 16), dtype=torch.uint8, device=self.device)
+        a, _ = self._ptrs()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        check(lib().bgk_dissipation(ctypes.byref(self.params), a, float(nu), self._out.data_ptr(), ws.data_ptr(),
+                                    ws.numel(), st), "bgk_dissipation")
+        return self._out[:7].cpu().numpy().copy()
+
     def draglift(self, box) -> np.ndarray:
         """FP64 momentum-exchange force (Fx, Fy, Fz) over the box (is, ie, js, je, ks, ke)."""
         ws = self._workspace()
@@ -230,7 +242,7 @@ class Lattice:
         check(self.L.bgk_lattice_load(self.h, st.ctypes.data, self._stream()), "bgk_lattice_load")
         torch.cuda.current_stream(self.device).synchronize()
 
-    FLOWS = {"uniform": 0, "rest": 0, "tgv": 1, "kida": 2}
+    FLOWS = {"uniform": 0, "rest": 0, "tgv": 1, "kida": 2, "tgv_ref": 3, "tg2d_ref": 4}
 
     def init_flow(self, flow: str, params=(1.0, 0.0, 0.0, 0.0)) -> None:
         """Equilibrium state of an analytic flow computed on the device."""
@@ -286,6 +298,11 @@ class Lattice:
     def step(self, nsteps=1) -> None:
         check(self.L.bgk_lattice_step(self.h, int(nsteps), self._stream()), "bgk_lattice_step")
 
+    def prepare(self) -> None:
+        """Capture the step graph now (nothing runs), so that the first long
+        step run starts without the capture."""
+        check(self.L.bgk_lattice_prepare(self.h), "bgk_lattice_prepare")
+
     def step_moments(self, nsteps: int, every: int = 1) -> np.ndarray:
         """Advance nsteps steps; FP64 moments of the state after every `every`-th
         step, computed in the same pass as that step: array (nsteps // every, 5)."""
@@ -302,6 +319,13 @@ class Lattice:
     def moments(self) -> np.ndarray:
         check(self.L.bgk_lattice_moments(self.h, self._out.data_ptr(), self._stream()), "moments")
         return self._out[:5].cpu().numpy().copy()
+
+    def dissipation(self, nu: float) -> np.ndarray:
+        """FP64 TKE, 2 nu Pi:Pi, mean squares, enstrophy and its node count
+        (bgk_lattice_dissipation), 7 values."""
+        check(self.L.bgk_lattice_dissipation(self.h, float(nu), self._out.data_ptr(), self._stream()),
+              "dissipation")
+        return self._out[:7].cpu().numpy().copy()
 
     def draglift(self, box) -> np.ndarray:
         check(self.L.bgk_lattice_draglift(self.h, *[int(v) for v in box], self._out.data_ptr(),

@@ -15,6 +15,9 @@
  *   bgk_moments    <- diagno            SRC/diagno.F90:87-138 (host/OpenACC
  *                                       reduction in the reference)
  *   bgk_draglift   <- draglift          SRC/draglift.F90:77-181
+ *   bgk_dissipation<- dissipation       SRC/dissipation.F90:25-350 (TKE and
+ *                                       2 nu Pi:Pi), plus the enstrophy of
+ *                                       the vorticity of SRC/vtk_om.xy.binary.F90
  *   bgk_profile    <- prof_i/_j/_k      SRC/prof_k.F90:47-87 (host loops
  *                                       after a full-state copy in the reference)
  *   bgk_probe      <- probe             SRC/probe.F90:50-78
@@ -123,11 +126,42 @@ int bgk_moments(const bgk_sweep_params* p, void* const* a, double* out_dev, void
    sums live in a 2 MiB device array inside the library (bgk_moments_noalloc_
    max_bytes()), held on every GPU that loads the library until exit; the
    device address is looked up on the first call on each device (make that
-   call before any stream capture).  Lattices whose reduction needs more
-   scratch than that are rejected with BGK_ERR_ARG.  Calls share the array:
-   calls that overlap on the GPU race.  Results are identical to bgk_moments. */
+   call before any stream capture) and kept until exit, so the entry point
+   must not be used on a device after a cudaDeviceReset of it.  Lattices
+   whose reduction needs more than 2 MiB (bgk_reduce_workspace_bytes(l, m, n)
+   = 40 B x ceil(l/tx) x ceil(m/ty) x min(n, 64) blocks, tx x ty = 256, tx the
+   smallest power of two >= l in 32..256: at most 52428 blocks, so 256^3 is
+   served and 512^3 is not) are rejected with BGK_ERR_ARG.  Calls share the
+   array: calls that overlap on the GPU race.  Results are identical to
+   bgk_moments bit for bit (the same launches with the same grid). */
 int bgk_moments_noalloc(const bgk_sweep_params* p, void* const* a, double* out_dev, void* stream);
 size_t bgk_moments_noalloc_max_bytes(void);
+
+/* FP64 turbulence diagnostics of the state in a (the routine dissipation of
+   SRC/dissipation.F90:25-350, called by SRC/diagnostic.F90:103), into
+   out_dev[0..6]:
+     [0] sum 0.5 |u|^2           (tke,  :177)
+     [1] sum 2 nu Pi:Pi          (diss, :338; Pi the non-equilibrium stress of
+                                  the pulled populations, :180-335)
+     [2..4] sum u_x^2, u_y^2, u_z^2   (vx2m, vy2m, vz2m, :172-174)
+     [5] sum 0.5 |w|^2, w = curl u by central differences of the node
+         velocities (the vorticity of SRC/vtk_om.xy.binary.F90:49-87)
+     [6] number of nodes in [5]
+   Sums over fluid nodes, per-node values in the compute type and the
+   reference's operation order, accumulated in FP64 (the reference
+   accumulates in mykind).  [0..4] pull every population from its upstream
+   neighbour as the reference does (:136-154), with the boundary case of p
+   resolved as bgk_sweep resolves it -- what the reference's pull reads
+   right after its boundary routines -- or, for BGK_BC_NONE, the halo as
+   stored; the inflow case writes the outflow halo plane first.  [5, 6]:
+   periodic axes of the case wrap; along other axes the two face layers are
+   left out; nodes that are solid or next to a solid are left out.  nu is
+   the kinematic viscosity (svisc); the caller normalises as the reference
+   writes dissipation.dat (divide by l m n u0^2).  Workspace:
+   bgk_dissipation_workspace_bytes(l, m, n) bytes. */
+size_t bgk_dissipation_workspace_bytes(int l, int m, int n);
+int bgk_dissipation(const bgk_sweep_params* p, void* const* a, double nu, double* out_dev, void* workspace,
+                    size_t workspace_bytes, void* stream);
 
 /* FP64 momentum-exchange force (Fx, Fy, Fz, unnormalised) on the obstacle,
    summed over fluid nodes in the box [is..ie]x[js..je]x[ks..ke]

@@ -84,8 +84,13 @@ int bgk_lattice_store(const bgk_lattice* lat, void* host, void* stream);
 /* Equilibrium initial state of an analytic flow computed on the device
    (SRC/init.F90:113-201 without the host): flow 0 uniform (params = rho,
    u_x, u_y, u_z; rest = 1,0,0,0), 1 Taylor-Green vortex (params[0] = u0;
-   x = 2 pi (i-1)/l, ...), 2 Kida vortex (params[0] = u0, rho = 1).  Resets the
-   step count like bgk_lattice_load. */
+   x = 2 pi (i-1)/l, ...), 2 Kida vortex (params[0] = u0, rho = 1) -- these
+   three in double, rounded once, keeping w_p (rho - 1) -- and the
+   reference's own forms in its arithmetic (compute type, its literals,
+   w_p (rho - 1) dropped as its shifted storage drops it): 3 the TGV3D form
+   (SRC/init.F90:141-148, x = (i - 0.5)/l, params[0] = u00), 4 the default
+   periodic 2-D Taylor-Green form (:125-130).  Resets the step count like
+   bgk_lattice_load. */
 int bgk_lattice_init(bgk_lattice* lat, int flow, const double* params, void* stream);
 
 /* Restart files in the reference's record format (SRC/save_raw.F90:37-69,
@@ -117,8 +122,15 @@ int bgk_lattice_restore(bgk_lattice* lat, const char* path, int* itime, void* st
 long long bgk_io_set_subrecord_limit(long long bytes);
 
 /* Advance nsteps time steps (boundaries + stream + collide), stream-ordered.
-   Runs of 16 or more steps replay a captured CUDA graph. */
+   Runs of 32 or more steps replay a captured 16-step CUDA graph (captured on
+   the first such run unless bgk_lattice_prepare captured it before). */
 int bgk_lattice_step(bgk_lattice* lat, int nsteps, void* stream);
+
+/* Capture the 16-step CUDA graph of bgk_lattice_step now, without running
+   it (no kernel executes and the state is untouched), so that the first long
+   step run launches at once.  A no-op when the graph exists.  No counterpart
+   in the reference. */
+int bgk_lattice_prepare(bgk_lattice* lat);
 
 /* Advance nsteps steps and record the FP64 moments (as bgk_moments) of the
    state after every `every`-th step, computed in the same pass as that step:
@@ -131,6 +143,11 @@ int bgk_lattice_set_omega(bgk_lattice* lat, double omega);
 /* FP64 moments (as bgk_moments) of the current state into out_dev[0..4];
    AA lattices need an even step count. */
 int bgk_lattice_moments(const bgk_lattice* lat, double* out_dev, void* stream);
+
+/* FP64 turbulence diagnostics (as bgk_dissipation) of the current state into
+   out_dev[0..6], with the lattice's boundary case; AA lattices need an even
+   step count. */
+int bgk_lattice_dissipation(const bgk_lattice* lat, double nu, double* out_dev, void* stream);
 
 /* FP64 drag/lift (as bgk_draglift) over the box into out_dev[0..2]. */
 int bgk_lattice_draglift(const bgk_lattice* lat, int is, int ie, int js, int je, int ks, int ke,

@@ -23,7 +23,23 @@
 //    * SRC/diagno.F90:87-138         per-node moments, FP64 accumulation
 //    * SRC/draglift.F90:77-176       momentum-exchange drag/lift (accumulated
 //                                   in FP64 here; the reference uses mykind)
-//    * SRC/dissipation.F90:136-300   tke / 2 nu Pi:Pi dissipation sums (FP64)
+//    * SRC/dissipation.F90:136-338   tke, 2 nu Pi:Pi dissipation and the mean
+//                                   squared velocity components (per-node in
+//                                   the compute type, sums in FP64; the
+//                                   reference sums in mykind), the pull read
+//                                   from the halo as stored
+//    * SRC/vtk_om.xy.binary.F90:49-87 node velocities and their central
+//                                   differences (the vorticity), summed here
+//                                   as the enstrophy 0.5 |w|^2 (FP64)
+//    * SRC/init.F90:113-201          initial populations: the TGV3D form and
+//                                   the default periodic 2-D Taylor-Green form,
+//                                   in mykind arithmetic with the reference's
+//                                   literals (pi is a default-real constant,
+//                                   0.1d0 promotes its products to double),
+//                                   shifted storage dropping w (rho - 1)
+//                                   (cte1 = 0); next to them the benchmark
+//                                   forms (uniform, Taylor-Green and Kida at
+//                                   2 pi (i-1)/l, in double, keeping w (rho - 1))
 //
 //  Storage kinds (kind argument):
 //    0  f64 storage, f64 compute      (DOUBLE)
@@ -45,6 +61,7 @@
 #include <cstring>
 #include <cmath>
 #include <cstdlib>
+#include <vector>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -168,6 +185,33 @@ template <class S, class C> struct SetSc {
 };
 template <> struct SetSc<Half, float> { static void set(Ctx<Half, float>& c) { c.sc = c.scl; } };
 template <> struct SetSc<BF16, float> { static void set(Ctx<BF16, float>& c) { c.sc = c.scl; } };
+
+// Velocity components of populations 01..19 (index 0..18), SRC/alloca.F90:29-148.
+inline int cx_tab(int p) {
+    static const int t[19] = {1, 1, 1, 1, 1, 0, 0, 0, 0, -1, -1, -1, -1, -1, 0, 0, 0, 0, 0};
+    return t[p];
+}
+inline int cy_tab(int p) {
+    static const int t[19] = {-1, 0, 1, 0, 0, 0, 1, 1, 1, -1, 0, 1, 0, 0, 0, -1, -1, -1, 0};
+    return t[p];
+}
+inline int cz_tab(int p) {
+    static const int t[19] = {0, -1, 0, 1, 0, 1, 1, 0, -1, 0, -1, 0, 1, 0, -1, -1, 0, 1, 0};
+    return t[p];
+}
+
+// A double rounded to storage kind S the way the library's initial-state
+// kernel rounds it: to float first for the 4- and 2-byte kinds, then (16-bit
+// kinds) times the power-of-two scale and to nearest even.
+template <class S> struct StoreD;
+template <> struct StoreD<double> { static double st(double v, const float*) { return v; } };
+template <> struct StoreD<float> { static float st(double v, const float*) { return (float)v; } };
+template <> struct StoreD<Half> {
+    static Half st(double v, const float* s) { return Half{float_to_half((float)v * s[0])}; }
+};
+template <> struct StoreD<BF16> {
+    static BF16 st(double v, const float* s) { return BF16{float_to_bf16((float)v * s[0])}; }
+};
 
 // ------------------------------------------------------ boundary conditions
 // SRC/bcond.periodic.F90:107-252 (x, then y, then z; full halo ranges)
@@ -578,6 +622,271 @@ void draglift(Ctx<S, C>& A, const int32_t* obs, int l, int m, int n, int is, int
     out[0] = F[0]; out[1] = F[1]; out[2] = F[2];
 }
 
+// SRC/dissipation.F90:136-338 over fluid nodes (obs == 1 skipped): each
+// population pulled from its upstream neighbour as stored (the caller fills
+// the halo first, as the reference's boundary routines do), rho and u, the
+// generic equilibrium e_p, n_p = x_p - e_p, the stress components and
+// Ptotal, all in the compute type in source order.  out = {sum 0.5*vsq,
+// sum 2*svisc*Ptotal, sum vx2, sum vy2, sum vz2} (FP64 sums).
+template <class S, class C>
+void dissipation(Ctx<S, C>& A, int l, int m, int n, const int32_t* obs, C svisc, C cte0, C cte1, C p0, C p1, C p2,
+                 C rf, C qf, C tre, double* out) {
+    const C due = C(2);
+    double diss = 0, tke = 0, vx2m = 0, vy2m = 0, vz2m = 0;
+    for (int k = 1; k <= n; ++k)
+        for (int j = 1; j <= m; ++j)
+            for (int i = 1; i <= l; ++i) {
+                if (obs && obs[(long)(i - 1) + (long)l * (j - 1) + (long)l * m * (k - 1)] == 1) continue;
+                const C x01 = A.ld(1, i - 1, j + 1, k);
+                const C x02 = A.ld(2, i - 1, j, k + 1);
+                const C x03 = A.ld(3, i - 1, j - 1, k);
+                const C x04 = A.ld(4, i - 1, j, k - 1);
+                const C x05 = A.ld(5, i - 1, j, k);
+                const C x06 = A.ld(6, i, j, k - 1);
+                const C x07 = A.ld(7, i, j - 1, k - 1);
+                const C x08 = A.ld(8, i, j - 1, k);
+                const C x09 = A.ld(9, i, j - 1, k + 1);
+                const C x10 = A.ld(10, i + 1, j + 1, k);
+                const C x11 = A.ld(11, i + 1, j, k + 1);
+                const C x12 = A.ld(12, i + 1, j - 1, k);
+                const C x13 = A.ld(13, i + 1, j, k - 1);
+                const C x14 = A.ld(14, i + 1, j, k);
+                const C x15 = A.ld(15, i, j, k + 1);
+                const C x16 = A.ld(16, i, j + 1, k + 1);
+                const C x17 = A.ld(17, i, j + 1, k);
+                const C x18 = A.ld(18, i, j + 1, k - 1);
+                const C x19 = A.ld(19, i, j, k);
+                const C rho = x01 + x02 + x03 + x04 + x05 + x06 + x07 + x08 + x09 + x10 + x11 + x12 + x13 + x14 +
+                              x15 + x16 + x17 + x18 + x19 + cte1;
+                const C rhoinv = C(1) / rho;
+                C vx = (x01 + x02 + x03 + x04 + x05 - x10 - x11 - x12 - x13 - x14) * rhoinv;
+                C vy = (x03 + x07 + x08 + x09 + x12 - x01 - x10 - x16 - x17 - x18) * rhoinv;
+                C vz = (x04 + x06 + x07 + x13 + x18 - x02 - x09 - x11 - x15 - x16) * rhoinv;
+                const C vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
+                vx2m += (double)vx2;
+                vy2m += (double)vy2;
+                vz2m += (double)vz2;
+                const C vsq = vx2 + vy2 + vz2;
+                tke += (double)(C(0.5) * vsq);
+                C vxpy = vx + vy;
+                const C qxpy = cte0 + qf * (tre * vxpy * vxpy - vsq);
+                C vxmy = vx - vy;
+                const C qxmy = cte0 + qf * (tre * vxmy * vxmy - vsq);
+                C vxpz = vx + vz;
+                const C qxpz = cte0 + qf * (tre * vxpz * vxpz - vsq);
+                C vxmz = vx - vz;
+                const C qxmz = cte0 + qf * (tre * vxmz * vxmz - vsq);
+                C vypz = vy + vz;
+                const C qypz = cte0 + qf * (tre * vypz * vypz - vsq);
+                C vymz = vy - vz;
+                const C qymz = cte0 + qf * (tre * vymz * vymz - vsq);
+                const C qx = cte0 + qf * (tre * vx2 - vsq);
+                const C qy = cte0 + qf * (tre * vy2 - vsq);
+                const C qz = cte0 + qf * (tre * vz2 - vsq);
+                vx = rf * vx; vy = rf * vy; vz = rf * vz;
+                vxpy = rf * vxpy; vxmy = rf * vxmy; vxpz = rf * vxpz;
+                vxmz = rf * vxmz; vypz = rf * vypz; vymz = rf * vymz;
+                const C rp1 = rho * p1, rp2 = rho * p2;
+                (void)p0;   // e19 enters no stress component
+                const C e01 = rp2 * (+vxmy + qxmy) + cte1 * (rp2 - p2);
+                const C e02 = rp2 * (+vxmz + qxmz) + cte1 * (rp2 - p2);
+                const C e03 = rp2 * (+vxpy + qxpy) + cte1 * (rp2 - p2);
+                const C e04 = rp2 * (+vxpz + qxpz) + cte1 * (rp2 - p2);
+                const C e05 = rp1 * (+vx + qx) + cte1 * (rp1 - p1);
+                const C e06 = rp1 * (+vz + qz) + cte1 * (rp1 - p1);
+                const C e07 = rp2 * (+vypz + qypz) + cte1 * (rp2 - p2);
+                const C e08 = rp1 * (+vy + qy) + cte1 * (rp1 - p1);
+                const C e09 = rp2 * (+vymz + qymz) + cte1 * (rp2 - p2);
+                const C e10 = rp2 * (-vxpy + qxpy) + cte1 * (rp2 - p2);
+                const C e11 = rp2 * (-vxpz + qxpz) + cte1 * (rp2 - p2);
+                const C e12 = rp2 * (-vxmy + qxmy) + cte1 * (rp2 - p2);
+                const C e13 = rp2 * (-vxmz + qxmz) + cte1 * (rp2 - p2);
+                const C e14 = rp1 * (-vx + qx) + cte1 * (rp1 - p1);
+                const C e15 = rp1 * (-vz + qz) + cte1 * (rp1 - p1);
+                const C e16 = rp2 * (-vypz + qypz) + cte1 * (rp2 - p2);
+                const C e17 = rp1 * (-vy + qy) + cte1 * (rp1 - p1);
+                const C e18 = rp2 * (-vymz + qymz) + cte1 * (rp2 - p2);
+                const C n01 = x01 - e01, n02 = x02 - e02, n03 = x03 - e03, n04 = x04 - e04, n05 = x05 - e05;
+                const C n06 = x06 - e06, n07 = x07 - e07, n08 = x08 - e08, n09 = x09 - e09, n10 = x10 - e10;
+                const C n11 = x11 - e11, n12 = x12 - e12, n13 = x13 - e13, n14 = x14 - e14, n15 = x15 - e15;
+                const C n16 = x16 - e16, n17 = x17 - e17, n18 = x18 - e18;
+                const C Pxx = n01 + n02 + n03 + n04 + n05 + n10 + n11 + n12 + n13 + n14;
+                const C Pyy = n01 + n03 + n07 + n08 + n09 + n10 + n12 + n16 + n17 + n18;
+                const C Pzz = n02 + n04 + n06 + n07 + n09 + n11 + n13 + n15 + n16 + n18;
+                const C Pxz = -n02 + n04 + n11 - n13;
+                const C Pxy = -n01 + n03 + n10 - n12;
+                const C Pyz = +n07 - n09 + n16 - n18;
+                const C Pyx = Pxy, Pzx = Pxz, Pzy = Pyz;
+                const C Ptotal = (Pxx * Pxx) + (Pyy * Pyy) + (Pzz * Pzz) + (due * Pxy * Pyx) + (due * Pxz * Pzx) +
+                                 (due * Pyz * Pzy);
+                diss += (double)(due * svisc * Ptotal);
+            }
+    out[0] = tke; out[1] = diss; out[2] = vx2m; out[3] = vy2m; out[4] = vz2m;
+}
+
+// Enstrophy: node velocities of the stored state as SRC/vtk_om.xy.binary.F90
+// :49-55 computes them (here in the compute type), central differences
+// du_a/dx_b = 0.5 (u_a(x + e_b) - u_a(x - e_b)) as :79-84, w = curl u as
+// :85-87, and the FP64 sum of 0.5 |w|^2.  Periodic axes (px, py, pz) wrap;
+// along other axes the two face layers are left out; with obs, nodes that
+// are solid or have a solid neighbour are left out.  out = {sum, nodes}.
+template <class S, class C>
+void enstrophy(Ctx<S, C>& A, int l, int m, int n, const int32_t* obs, C cte1, bool px, bool py, bool pz,
+               double* out) {
+    const long nn = (long)l * m * n;
+    std::vector<C> u(nn), v(nn), w(nn);
+    auto at = [&](int i, int j, int k) -> long { return (long)(i - 1) + (long)l * (j - 1) + (long)l * m * (k - 1); };
+    for (int k = 1; k <= n; ++k)
+        for (int j = 1; j <= m; ++j)
+            for (int i = 1; i <= l; ++i) {
+                C x[19];
+                for (int p = 0; p < 19; ++p) x[p] = A.ld(p + 1, i, j, k);
+                const C rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] + x[11] +
+                              x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18] + cte1;
+                const C rhoinv = C(1) / rho;
+                u[at(i, j, k)] = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * rhoinv;
+                v[at(i, j, k)] = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * rhoinv;
+                w[at(i, j, k)] = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * rhoinv;
+            }
+    auto wrap = [](int c, int len) { return c < 1 ? c + len : (c > len ? c - len : c); };
+    auto solid = [&](int i, int j, int k) { return obs && obs[at(i, j, k)] == 1; };
+    double sum = 0, cnt = 0;
+    const C h = C(0.5);
+    for (int k = 1; k <= n; ++k)
+        for (int j = 1; j <= m; ++j)
+            for (int i = 1; i <= l; ++i) {
+                if (!px && (i < 2 || i > l - 1)) continue;
+                if (!py && (j < 2 || j > m - 1)) continue;
+                if (!pz && (k < 2 || k > n - 1)) continue;
+                const int im = wrap(i - 1, l), ip = wrap(i + 1, l), jm = wrap(j - 1, m), jp = wrap(j + 1, m);
+                const int km = wrap(k - 1, n), kp = wrap(k + 1, n);
+                if (solid(i, j, k) || solid(im, j, k) || solid(ip, j, k) || solid(i, jm, k) || solid(i, jp, k) ||
+                    solid(i, j, km) || solid(i, j, kp))
+                    continue;
+                const C dudy = h * (u[at(i, jp, k)] - u[at(i, jm, k)]);
+                const C dudz = h * (u[at(i, j, kp)] - u[at(i, j, km)]);
+                const C dvdx = h * (v[at(ip, j, k)] - v[at(im, j, k)]);
+                const C dvdz = h * (v[at(i, j, kp)] - v[at(i, j, km)]);
+                const C dwdx = h * (w[at(ip, j, k)] - w[at(im, j, k)]);
+                const C dwdy = h * (w[at(i, jp, k)] - w[at(i, jm, k)]);
+                const C ox = dvdz - dwdy, oy = dwdx - dudz, oz = dudy - dvdx;
+                sum += (double)(h * (ox * ox + oy * oy + oz * oz));
+                cnt += 1.0;
+            }
+    out[0] = sum; out[1] = cnt;
+}
+
+// ------------------------------------------------------- initial state
+// Sine and cosine of the compute type as the reference calls them (sin/cos
+// of real(8); for real(4) the correctly rounded single-precision value --
+// libm's sinf/cosf, which the reference calls, agree with it except in rare
+// last-bit cases).
+inline float rsin(float a) { return (float)std::sin((double)a); }
+inline double rsin(double a) { return std::sin(a); }
+inline float rcos(float a) { return (float)std::cos((double)a); }
+inline double rcos(double a) { return std::cos(a); }
+
+// The 19 reference populations of SRC/init.F90:158-197 from (crho, xj, yj,
+// zj) in the compute type, with cte1 = 0 (shifted storage: no NOSHIFT):
+// f_p = crho * w_p * (cte1 + cx_p).
+template <class C>
+void init_pops_reference(C crho, C xj, C yj, C zj, C rf, C qf, C tre, C p0, C p1, C p2, C (&f)[19]) {
+    const C cte1 = C(0);
+    const C cvsq = xj * xj + yj * yj + zj * zj;
+    const C cx01 = rf * (xj - yj) + qf * (tre * (xj - yj) * (xj - yj) - cvsq);
+    const C cx02 = rf * (xj - zj) + qf * (tre * (xj - zj) * (xj - zj) - cvsq);
+    const C cx03 = rf * (xj + yj) + qf * (tre * (xj + yj) * (xj + yj) - cvsq);
+    const C cx04 = rf * (xj + zj) + qf * (tre * (xj + zj) * (xj + zj) - cvsq);
+    const C cx05 = rf * (xj) + qf * (tre * (xj) * (xj) - cvsq);
+    const C cx06 = rf * (zj) + qf * (tre * (zj) * (zj) - cvsq);
+    const C cx07 = rf * (yj + zj) + qf * (tre * (yj + zj) * (yj + zj) - cvsq);
+    const C cx08 = rf * (yj) + qf * (tre * (yj) * (yj) - cvsq);
+    const C cx09 = rf * (yj - zj) + qf * (tre * (yj - zj) * (yj - zj) - cvsq);
+    const C cx10 = rf * (-xj - yj) + qf * (tre * (xj + yj) * (xj + yj) - cvsq);
+    const C cx11 = rf * (-xj - zj) + qf * (tre * (xj + zj) * (xj + zj) - cvsq);
+    const C cx12 = rf * (-xj + yj) + qf * (tre * (xj - yj) * (xj - yj) - cvsq);
+    const C cx13 = rf * (-xj + zj) + qf * (tre * (xj - zj) * (xj - zj) - cvsq);
+    const C cx14 = rf * (-xj) + qf * (tre * (xj) * (xj) - cvsq);
+    const C cx15 = rf * (-zj) + qf * (tre * (zj) * (zj) - cvsq);
+    const C cx16 = rf * (-yj - zj) + qf * (tre * (yj + zj) * (yj + zj) - cvsq);
+    const C cx17 = rf * (-yj) + qf * (tre * (yj) * (yj) - cvsq);
+    const C cx18 = rf * (-yj + zj) + qf * (tre * (yj - zj) * (yj - zj) - cvsq);
+    const C cx19 = rf * C(0) + qf * (tre * C(0) * C(0) - cvsq);
+    const C cx[19] = {cx01, cx02, cx03, cx04, cx05, cx06, cx07, cx08, cx09, cx10,
+                      cx11, cx12, cx13, cx14, cx15, cx16, cx17, cx18, cx19};
+    for (int p = 0; p < 19; ++p) {
+        const int ax = std::abs(cx_tab(p)) + std::abs(cy_tab(p)) + std::abs(cz_tab(p));
+        const C w = ax == 0 ? p0 : (ax == 1 ? p1 : p2);
+        f[p] = crho * w * (cte1 + cx[p]);
+    }
+}
+
+// flow 0 uniform (prm = rho, ux, uy, uz), 1 Taylor-Green and 2 Kida at
+// x = 2 pi (i-1)/l (prm[0] = u0): w (rho - 1) + w rho (3 c.u + 4.5 (c.u)^2 -
+// 1.5 u^2) in double, rounded once to the storage kind.  flow 3: the
+// reference's TGV3D form (SRC/init.F90:119-158, prm[0] = u00), flow 4: its
+// default periodic 2-D Taylor-Green form (:125-130): x = (i - 0.5)/l in
+// double rounded to mykind, the rest in mykind.  Every node of the box
+// 0..l+1, 0..m+1, 0..n+1 is written.
+template <class S, class C>
+void init_state(Ctx<S, C>& A, int l, int m, int n, int flow, const double* prm, C rf, C qf, C tre, C p0, C p1,
+                C p2) {
+    const double tp = 6.283185307179586476925286766559;
+    const C pi = C(3.14159265358979323846f);   // a default-real literal (SRC/init.F90:63)
+    for (int k = 0; k <= n + 1; ++k)
+        for (int j = 0; j <= m + 1; ++j)
+            for (int i = 0; i <= l + 1; ++i) {
+                if (flow <= 2) {
+                    double rho = 1.0, ux = 0.0, uy = 0.0, uz = 0.0;
+                    if (flow == 0) {
+                        rho = prm[0]; ux = prm[1]; uy = prm[2]; uz = prm[3];
+                    } else {
+                        const double x = tp * (i - 1) / l, y = tp * (j - 1) / m, z = tp * (k - 1) / n;
+                        const double u0 = prm[0];
+                        if (flow == 1) {
+                            ux = u0 * std::sin(x) * std::cos(y) * std::cos(z);
+                            uy = -u0 * std::cos(x) * std::sin(y) * std::cos(z);
+                            rho = 1.0 + 3.0 * (u0 * u0 / 16.0) * (std::cos(2.0 * x) + std::cos(2.0 * y)) *
+                                            (std::cos(2.0 * z) + 2.0);
+                        } else {
+                            ux = u0 * std::sin(x) * (std::cos(3.0 * y) * std::cos(z) - std::cos(y) * std::cos(3.0 * z));
+                            uy = u0 * std::sin(y) * (std::cos(3.0 * z) * std::cos(x) - std::cos(z) * std::cos(3.0 * x));
+                            uz = u0 * std::sin(z) * (std::cos(3.0 * x) * std::cos(y) - std::cos(x) * std::cos(3.0 * y));
+                        }
+                    }
+                    const double usq = ux * ux + uy * uy + uz * uz;
+                    for (int p = 0; p < 19; ++p) {
+                        const double cu = cx_tab(p) * ux + cy_tab(p) * uy + cz_tab(p) * uz;
+                        const int ax = std::abs(cx_tab(p)) + std::abs(cy_tab(p)) + std::abs(cz_tab(p));
+                        const double w = ax == 2 ? 1.0 / 36.0 : (ax == 1 ? 1.0 / 18.0 : 1.0 / 3.0);
+                        const double v = w * (rho - 1.0) + w * rho * (3.0 * cu + 4.5 * cu * cu - 1.5 * usq);
+                        A.at(p + 1, i, j, k) = StoreD<S>::st(v, A.scl);
+                    }
+                    continue;
+                }
+                const C x = (C)(((double)i - 0.5) / (double)l);
+                const C y = (C)(((double)j - 0.5) / (double)m);
+                const C z = (C)(((double)k - 0.5) / (double)n);
+                C xj, yj, zj, crho = C(1);
+                if (flow == 3) {
+                    const C u00 = (C)prm[0], due = C(2), qua = C(4);
+                    xj = u00 * rsin(due * pi * x) * rcos(due * pi * y) * rcos(due * pi * z);
+                    yj = -(u00 * rcos(due * pi * x) * rsin(due * pi * y) * rcos(due * pi * z));
+                    zj = C(0);
+                    crho = C(1) + ((u00 * u00) / (qua * qua * tre)) * (rcos(qua * pi * x) + rcos(qua * pi * y)) *
+                                      (rcos(qua * pi * z) + due);
+                } else {
+                    const C two = C(2);
+                    xj = (C)(0.1 * (double)rsin(two * pi * x) * (double)rcos(two * pi * z));
+                    yj = C(0);
+                    zj = (C)(-(0.1 * (double)rcos(two * pi * x) * (double)rsin(two * pi * z)));
+                }
+                C f[19];
+                init_pops_reference<C>(crho, xj, yj, zj, rf, qf, tre, p0, p1, p2, f);
+                for (int p = 0; p < 19; ++p) A.st(p + 1, i, j, k, f[p]);
+            }
+}
+
 // ------------------------------------------------- profiles, probe, slices
 // The storage arithmetic: the reference sums the storage arrays directly in
 // these routines, so the arithmetic is the storage kind's (float for the
@@ -748,6 +1057,38 @@ int orc_slice(int kind, void** a, int l, int m, int n, int nx, int ny, int plane
     DISPATCH(kind, {
         Ctx<S, C> A; make(A, a, nx, ny, scale);
         slice(A, plane, index, l, m, n, out);
+    });
+    return 0;
+}
+
+// out[0..4]: dissipation sums (see dissipation above); the halo as stored.
+int orc_dissipation(int kind, void** a, int l, int m, int n, int nx, int ny, const int32_t* obs, double svisc,
+                    double cte0, double cte1, double p0, double p1, double p2, double rf, double qf, double tre,
+                    const float* scale, double* out) {
+    DISPATCH(kind, {
+        Ctx<S, C> A; make(A, a, nx, ny, scale);
+        dissipation(A, l, m, n, obs, (C)svisc, (C)cte0, (C)cte1, (C)p0, (C)p1, (C)p2, (C)rf, (C)qf, (C)tre, out);
+    });
+    return 0;
+}
+
+// out[0..1]: enstrophy sum and node count; periodic: bit 0 x, bit 1 y, bit 2 z.
+int orc_enstrophy(int kind, void** a, int l, int m, int n, int nx, int ny, const int32_t* obs, double cte1,
+                  int periodic, const float* scale, double* out) {
+    DISPATCH(kind, {
+        Ctx<S, C> A; make(A, a, nx, ny, scale);
+        enstrophy(A, l, m, n, obs, (C)cte1, (periodic & 1) != 0, (periodic & 2) != 0, (periodic & 4) != 0, out);
+    });
+    return 0;
+}
+
+// The initial state of `flow` (see init_state) over the whole box.
+int orc_init(int kind, void** a, int l, int m, int n, int nx, int ny, int flow, const double* prm, double rf,
+             double qf, double tre, double p0, double p1, double p2, const float* scale) {
+    if (flow < 0 || flow > 4) return -2;
+    DISPATCH(kind, {
+        Ctx<S, C> A; make(A, a, nx, ny, scale);
+        init_state(A, l, m, n, flow, prm, (C)rf, (C)qf, (C)tre, (C)p0, (C)p1, (C)p2);
     });
     return 0;
 }

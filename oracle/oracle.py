@@ -55,6 +55,9 @@ def lib() -> ctypes.CDLL:
         L.orc_profile.argtypes = [c_int, pp] + [c_int] * 8 + [c_double, fp, dp]
         L.orc_probe.argtypes = [c_int, pp] + [c_int] * 5 + [c_double, fp, dp]
         L.orc_slice.argtypes = [c_int, pp] + [c_int] * 7 + [fp, fp]
+        L.orc_dissipation.argtypes = [c_int, pp] + [c_int] * 5 + [c_void_p] + [c_double] * 9 + [fp, dp]
+        L.orc_enstrophy.argtypes = [c_int, pp] + [c_int] * 5 + [c_void_p, c_double, c_int, fp, dp]
+        L.orc_init.argtypes = [c_int, pp] + [c_int] * 6 + [dp] + [c_double] * 6 + [fp]
         L.orc_float_to_half.argtypes = [c_float]
         L.orc_float_to_half.restype = ctypes.c_uint16
         L.orc_half_to_float.argtypes = [ctypes.c_uint16]
@@ -158,6 +161,42 @@ class OracleLattice:
                               obs, cte1, self.scale, out)
         assert rc == 0
         return np.array(out[:])
+
+    def dissipation(self, svisc, cte1=1.0, p0=1.0 / 3.0, p1=1.0 / 18.0, p2=1.0 / 36.0, rf=3.0, qf=1.5,
+                    tre=3.0, fluid_only=True) -> np.ndarray:
+        """SRC/dissipation.F90:136-338 on the current a arrays, halo as stored
+        (call bcond first for the reference's boundary values): {sum 0.5 vsq,
+        sum 2 nu Ptotal, sum vx2, sum vy2, sum vz2}."""
+        out = (c_double * 5)()
+        obs = self.obs.ctypes.data if (fluid_only and self.obs is not None) else None
+        rc = lib().orc_dissipation(self.kind, _ptrs(self.a), self.l, self.m, self.n, self.nx, self.ny, obs,
+                                   svisc, 1.0 - cte1, cte1, p0, p1, p2, rf, qf, tre, self.scale, out)
+        assert rc == 0
+        return np.array(out[:])
+
+    def enstrophy(self, periodic=(True, True, True), cte1=1.0) -> np.ndarray:
+        """{sum 0.5 |curl u|^2, nodes counted} with central differences of the
+        node velocities (SRC/vtk_om.xy.binary.F90:49-87); periodic axes wrap,
+        other axes leave out their two face layers."""
+        out = (c_double * 2)()
+        obs = self.obs.ctypes.data if self.obs is not None else None
+        bits = sum(1 << a for a, p in enumerate(periodic) if p)
+        rc = lib().orc_enstrophy(self.kind, _ptrs(self.a), self.l, self.m, self.n, self.nx, self.ny, obs, cte1,
+                                 bits, self.scale, out)
+        assert rc == 0
+        return np.array(out[:])
+
+    def init(self, flow: int, params=(1.0, 0.0, 0.0, 0.0), rf=3.0, qf=1.5, tre=3.0, p0=1.0 / 3.0,
+             p1=1.0 / 18.0, p2=1.0 / 36.0) -> None:
+        """Initial populations over the whole box: flow 0 uniform, 1 Taylor-Green,
+        2 Kida (benchmark forms), 3 the reference's TGV3D form, 4 its default
+        periodic 2-D Taylor-Green form (SRC/init.F90:113-201)."""
+        prm = (c_double * 4)(*([float(v) for v in params] + [0.0] * (4 - len(params))))
+        rc = lib().orc_init(self.kind, _ptrs(self.a), self.l, self.m, self.n, self.nx, self.ny, flow, prm,
+                            rf, qf, tre, p0, p1, p2, self.scale)
+        assert rc == 0
+        for d in range(18):
+            self.b[d][...] = self.a[d]
 
     def draglift(self, box) -> np.ndarray:
         out = (c_double * 3)()

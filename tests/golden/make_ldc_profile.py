@@ -20,7 +20,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT = "/root/reference/TEST/DrivenCavity/OFFLOAD_256/prof_k.dat"
+# the reference checkout's root from BGK3D_REFERENCE, when no path is given
+DEFAULT = os.path.join(os.environ.get("BGK3D_REFERENCE", "."), "TEST", "DrivenCavity", "OFFLOAD_256",
+                       "prof_k.dat")
 
 
 def parse(text: str):

@@ -1,52 +1,66 @@
-"""On-device initial conditions (bgk_lattice_init): the equilibrium state of an
-analytic flow computed by the init kernel must match the float64 numpy
-equilibrium of the same fields (SRC/init.F90:113-201, keeping the w (rho - 1)
-term) to within one rounding of the storage kind, for both access patterns,
-and a solve started from it must track the solve started from the uploaded
-host state."""
+"""On-device initial conditions (bgk_lattice_init) against the CPU oracle's
+restatement of SRC/init.F90:113-201: the reference's own TGV3D and default
+2-D Taylor-Green forms in its arithmetic (x = (i - 0.5)/l, its literals,
+w (rho - 1) dropped as its shifted storage drops it) and the benchmark forms
+(uniform, Taylor-Green and Kida at 2 pi (i-1)/l, double arithmetic, w (rho -
+1) kept), for every storage kind and both access patterns.  The two sides
+evaluate sine and cosine with different libraries (CUDA's and libm's), so
+each stored value may sit one storage rounding apart: the bit patterns, read
+as ordered integers, differ by at most 1.  A solve started from the device
+state must also track one started from the uploaded host state."""
 import numpy as np
 import pytest
-
-from bgk3d_gpu_b200 import fields as F
 
 from _cases import SCALE, interior
 
 pytestmark = pytest.mark.gpu
 
-# tolerance: one unit in the last place of the storage kind, relative to the
-# largest stored magnitude, plus a float64 allowance for sin/cos differences
-ULP = {0: 1e-14, 1: 2.0 ** -23, 2: 2.0 ** -10, 3: 2.0 ** -7, 4: 2.0 ** -23}
+FLOWS = {"uniform": 0, "tgv": 1, "kida": 2, "tgv_ref": 3, "tg2d_ref": 4}
 
 
-def _fields(flow, l, m, n, u0):
-    if flow == "tgv":
-        return F.taylor_green_fields(l, m, n, u0)
-    if flow == "kida":
-        return F.kida_fields(l, m, n, u0)
-    z = np.zeros((n, m, l))
-    return z + 1.02, z + 0.03, z - 0.01, z + 0.005
+def _ordered(bits: np.ndarray) -> np.ndarray:
+    """Storage bit patterns as integers that count representable values."""
+    if bits.dtype == np.float64:
+        u = bits.view(np.int64)
+        return np.where(u < 0, -(u & 0x7fffffffffffffff), u)
+    if bits.dtype == np.float32:
+        u = bits.view(np.int32).astype(np.int64)
+        return np.where(u < 0, -(u & 0x7fffffff), u)
+    u = bits.astype(np.int64)   # uint16 patterns of f16 / bf16
+    return np.where(u & 0x8000, -(u & 0x7fff), u)
 
 
-def _expected(flow, l, m, n, u0):
-    rho, ux, uy, uz = (np.asarray(v) for v in _fields(flow, l, m, n, u0))
-    return F.equilibrium_shifted(rho, ux, uy, uz)
+def _oracle_init(kind, l, m, n, flow, params):
+    from oracle.oracle import OracleLattice
+    o = OracleLattice(l, m, n, kind, scale=SCALE[kind])
+    o.init(FLOWS[flow], params)
+    return o.state()
 
 
 @pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("pattern", ["ab", "aa"])
-@pytest.mark.parametrize("flow", ["tgv", "kida", "uniform"])
-def test_device_init_matches_host_equilibrium(kind, pattern, flow):
+@pytest.mark.parametrize("flow", list(FLOWS))
+def test_device_init_matches_oracle(kind, pattern, flow):
     from bgk3d_gpu_b200.lattice import Lattice
     l, m, n, u0 = 24, 20, 16, 0.05
     lat = Lattice(l, m, n, kind=kind, bcase="periodic", omega=1.6, pattern=pattern, scale=SCALE[kind])
-    params = (u0,) if flow != "uniform" else (1.02, 0.03, -0.01, 0.005)
+    params = (1.02, 0.03, -0.01, 0.005) if flow == "uniform" else (u0,)
     lat.init_flow(flow, params)
     assert lat.steps == 0
-    got = F.from_storage_bits(interior(lat.download(), l, m, n), kind, SCALE[kind])
-    want = _expected(flow, l, m, n, u0)
-    tol = ULP[kind] * np.abs(want).max() + 1e-15
-    assert np.abs(got - want).max() <= tol, (kind, pattern, flow, np.abs(got - want).max(), tol)
+    got = interior(lat.download(), l, m, n)
+    want = interior(_oracle_init(kind, l, m, n, flow, params), l, m, n)
     lat.close()
+    if kind == 0:
+        # FP64 storage keeps the libraries' last-bit sine differences
+        # (CUDA's double sin is within 2 units, libm's within 1): a few
+        # units of the largest value
+        tol = 16 * 2.0 ** -52 * np.abs(want).max()
+        assert np.abs(got - want).max() <= tol, (pattern, flow, np.abs(got - want).max(), tol)
+        return
+    d = np.abs(_ordered(np.ascontiguousarray(got)) - _ordered(np.ascontiguousarray(want)))
+    assert d.max() <= 1, (kind, pattern, flow, int(d.max()), int((d > 0).sum()))
+    # most values agree bit for bit; the rest sit on a rounding boundary
+    assert (d == 0).mean() > 0.9, (kind, pattern, flow, float((d == 0).mean()))
 
 
 @pytest.mark.parametrize("kind", [1, 2])

@@ -8,8 +8,8 @@ that reserves its whole memory budget up front and allows no allocation in
 its time loop.  It keeps its scratch in a fixed device array inside the
 library.  These tests call it through the C ABI twice in a row (the second
 call finds the first call's partial sums still in that array) and compare
-with bgk_moments at the tolerance of the other reduction tests.  The file
-is named to be collected last.
+with bgk_moments: both run the same two launches with the same grid, so the
+sums must be identical bit for bit.  The file is named to be collected last.
 """
 import ctypes
 
@@ -45,7 +45,7 @@ def test_noalloc_matches_workspace_moments_twice(kind):
     for call in range(2):
         want = lat.moments()
         got = _noalloc(lat, L)
-        np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-12)
+        assert np.array_equal(got, want), (got, want)
         lat.step(1)   # new data for the second call; the scratch still holds the first call's sums
 
 
@@ -61,3 +61,55 @@ def test_noalloc_rejects_lattice_beyond_its_scratch():
     rc = L.bgk_moments_noalloc(ctypes.byref(p), dummy, ctypes.c_void_p(256), None)
     assert rc == _lib.BGK_ERR_ARG
     assert "at most" in L.bgk_last_error().decode()
+
+
+def _grid_blocks(l, m, n):
+    """Blocks of the moments pass: ceil(l/tx) x ceil(m/ty) x min(n, 64), with
+    tx the smallest power of two >= l in 32..256 and ty = 256 / tx."""
+    tx = 32
+    while tx < l and tx < 256:
+        tx *= 2
+    ty = 256 // tx
+    return -(-l // tx) * -(-m // ty) * min(n, 64)
+
+
+def test_noalloc_bound_is_the_documented_one():
+    """40 bytes of partial sums per block of the moments pass: 2 MiB hold
+    52428 blocks.  256^3 fits (16384 blocks); 512^3 (65536 blocks) and
+    512 x 512 x 64 do not."""
+    from bgk3d_gpu_b200 import _lib
+    L = _lib.lib()
+    cap = L.bgk_moments_noalloc_max_bytes()
+    for shape in [(256, 256, 256), (256, 819, 64), (256, 820, 64), (512, 512, 64), (512, 512, 512), (40, 36, 30)]:
+        assert L.bgk_reduce_workspace_bytes(*shape) == 40 * _grid_blocks(*shape)
+    assert cap // 40 == 52428
+    assert _grid_blocks(256, 256, 256) == 16384 and 40 * 16384 <= cap
+    assert _grid_blocks(256, 819, 64) == 52416 and L.bgk_reduce_workspace_bytes(256, 819, 64) <= cap
+    assert L.bgk_reduce_workspace_bytes(256, 820, 64) > cap
+    assert L.bgk_reduce_workspace_bytes(512, 512, 64) > cap
+    dummy = _lib.ptr_array([256] * 19)
+    for shape in [(512, 512, 64), (256, 820, 64)]:
+        p = _lib.sweep_params(_lib.KIND_F32, *shape, OMEGA)
+        assert L.bgk_moments_noalloc(ctypes.byref(p), dummy, ctypes.c_void_p(256), None) == _lib.BGK_ERR_ARG
+
+
+def test_noalloc_largest_accepted_lattice():
+    """The largest lattice shape of this family that the scratch holds
+    (256 x 819 x 64: 52416 of 52428 blocks), twice, bit for bit against
+    bgk_moments; the state is random data written on the device."""
+    import torch
+    from bgk3d_gpu_b200 import _lib
+    from bgk3d_gpu_b200.lattice import DeviceLattice
+    L = _lib.lib()
+    l, m, n = 256, 819, 64
+    lat = DeviceLattice(l, m, n, kind=1, bcase="periodic", omega=OMEGA)
+    g = torch.Generator(device=lat.device)
+    g.manual_seed(5)
+    for call in range(2):
+        for t in lat._a:
+            t.uniform_(-0.01, 0.01, generator=g)
+        want = lat.moments()
+        got = _noalloc(lat, L)
+        assert np.array_equal(got, want), (got, want)
+    del lat
+    torch.cuda.empty_cache()
