@@ -31,6 +31,16 @@ def bind_batch(L) -> None:
     L.bgk_batch_step.restype = c_int
     L.bgk_batch_set_config.argtypes = [c_void_p, c_int, c_int]
     L.bgk_batch_set_config.restype = c_int
+    L.bgk_batch_set_chunk.argtypes = [c_void_p, c_int]
+    L.bgk_batch_set_chunk.restype = c_int
+    L.bgk_batch_get_chunk.argtypes = [c_void_p, P_(c_int)]
+    L.bgk_batch_get_chunk.restype = c_int
+    L.bgk_batch_set_solo.argtypes = [c_void_p, c_longlong]
+    L.bgk_batch_set_solo.restype = c_int
+    L.bgk_batch_get_solo.argtypes = [c_void_p]
+    L.bgk_batch_get_solo.restype = c_longlong
+    L.bgk_batch_groups.argtypes = [c_void_p]
+    L.bgk_batch_groups.restype = c_int
     L.bgk_batch_get_config.argtypes = [c_void_p, P_(c_int), P_(c_int)]
     L.bgk_batch_get_config.restype = c_int
     L.bgk_batch_tune.argtypes = [c_void_p, c_int, c_void_p, P_(c_int)]

@@ -6,8 +6,10 @@ Poiseuille channel (x, y periodic, z walls, body force g = 1e-6 as g/10 per
 population with c_x != 0, times rho); FP32; `steps` steps each.
 
 Four ways to run the same solves are timed (CUDA events):
-  batched     one persistent tile-queue launch per step for all lattices,
-              16-step CUDA graphs, tile shape / grid chosen by the autotuner;
+  batched     the batch (bgk_batch_*): one launch per group of lattices that
+              share boundary case and collision mode (chunks of warp
+              segments per block) or one persistent tile-queue launch for
+              all, whichever the autotuner picks; 8-step CUDA graphs;
   sequential  one lattice after another, each with its own launches replayed
               through that lattice's CUDA graph;
   streams     the lattices' graphs on 8 side streams, side by side;
@@ -68,7 +70,7 @@ def timed(fn):
 
 
 def run(count: int = 96, steps: int = 2000, seed: int = 20261203, modes=("batched", "sequential", "plain"),
-        tune_steps: int = 4, side_set=SIDES):
+        tune_steps: int = 16, side_set=SIDES, chunk: int | None = None, solo: int | None = None):
     specs = make_specs(count, seed, side_set)
     lats, states = build(specs)
     nodes = sum(c["l"] * c["m"] * c["n"] for c in specs)
@@ -78,9 +80,16 @@ def run(count: int = 96, steps: int = 2000, seed: int = 20261203, modes=("batche
     finals = None
     if "batched" in modes:
         batch = Batch(lats)
-        used = batch.tune(tune_steps)
+        if chunk is None:
+            used = batch.tune(tune_steps)
+        else:
+            batch.set_chunk(chunk)
+            batch.set_solo(solo or 0)
+            used = 0
         cfg = batch.config
-        out["tuned_config"] = {"tiles_per_grab": cfg[0], "blocks_per_sm": cfg[1], "tuning_steps": used}
+        out["tuned_config"] = {"warps_per_chunk": batch.chunk, "launches_per_step": batch.groups,
+                               "solo_min_nodes": batch.solo,
+                               "tiles_per_grab": cfg[0], "blocks_per_sm": cfg[1], "tuning_steps": used}
         reload(lats, states)
         batch.resync()
         t = timed(lambda: batch.step(steps))
@@ -148,9 +157,13 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--modes", default="batched,sequential,streams,plain")
     ap.add_argument("--sides", default=",".join(str(v) for v in SIDES), help="cube sides drawn from")
+    ap.add_argument("--chunk", type=int, default=None,
+                    help="warp segments per chunk of the grouped form, no autotuning (0: tile queue)")
+    ap.add_argument("--solo", type=int, default=None,
+                    help="with --chunk: members of this many nodes or more step with their own launch")
     args = ap.parse_args(argv)
     res = run(args.count, args.steps, args.seed, tuple(args.modes.split(",")),
-              side_set=tuple(int(v) for v in args.sides.split(",")))
+              side_set=tuple(int(v) for v in args.sides.split(",")), chunk=args.chunk, solo=args.solo)
     print(json.dumps(res), flush=True)
     return 0
 

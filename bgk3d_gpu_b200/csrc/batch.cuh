@@ -115,4 +115,34 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) batch_grid_kernel
     batch_node<S, C>(P, (t - __ldg(V.tile_begin + lo)) * 8u + (threadIdx.x >> 5));
 }
 
+// Grouped form (the default): the members that share a boundary case,
+// collision mode and obstacle logic form a group, and each group is one
+// launch of a kernel compiled for exactly that variant -- no run-time
+// dispatch, no obstacle code in obstacle-free groups.  The host cuts every
+// member's step into chunks of chunk_warps consecutive warp segments and
+// lists them (member, first warp) in a table, so a block finds its work with
+// one load: it stages the member's kernel arguments in shared memory (the
+// block's only barrier) and its 8 warps then stride through the chunk's warp
+// segments with the per-node code of sweep_ab_kernel.  The hardware block
+// scheduler is the queue.
+template <class S, class C> struct BatchGroupView {
+    const SweepArgs<S, C>* desc;   // 2 per member of the batch: [2 member + parity]
+    const uint2* chunks;           // (member, first warp segment) per chunk of this group
+    int parity;
+    uint32_t chunk_warps;          // warp segments per chunk
+};
+
+template <class S, class C, int BC, int CM, bool OBS>
+__global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) batch_chunk_kernel(const BatchGroupView<S, C> V) {
+    __shared__ __align__(16) SweepArgs<S, C> sd;
+    const uint2 ch = V.chunks[blockIdx.x];
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(V.desc + 2 * ch.x + V.parity);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+    for (uint32_t w = threadIdx.x; w < sizeof(SweepArgs<S, C>) / 4; w += blockDim.x) dst[w] = __ldg(src + w);
+    __syncthreads();
+    double m5[5];
+    const uint32_t end = min(ch.y + V.chunk_warps, sd.nwarps);
+    for (uint32_t gw = ch.y + (threadIdx.x >> 5); gw < end; gw += 8u) sweep_node<S, C, BC, int, CM, OBS>(sd, gw, m5);
+}
+
 }  // namespace bgk

@@ -31,6 +31,9 @@ template <class S, class C>
 int launch_dissipation(const bgk_sweep_params* p, void* const* a, double nu, double* out, double* ws,
                        cudaStream_t st);
 template <class S, class C>
+int launch_batch_group(const void* desc, const void* chunks, uint32_t nchunks, uint32_t chunk_warps, int parity,
+                       int bcase, int cm, bool obs, cudaStream_t st);
+template <class S, class C>
 int launch_outflow(const bgk_sweep_params* p, void* const* a, cudaStream_t st);
 template <class S, class C>
 int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n, int flow, const double* prm,

@@ -431,6 +431,47 @@ int launch_batch(const void* desc, const uint32_t* tile_begin, int nlat, uint32_
     return check_launch("batch_sweep_kernel");
 }
 
+template <class S, class C, int BC, int CM>
+void launch_group_bc_cm(const BatchGroupView<S, C>& V, uint32_t nchunks, bool obs, cudaStream_t st) {
+    if (obs) batch_chunk_kernel<S, C, BC, CM, true><<<nchunks, 256, 0, st>>>(V);
+    else batch_chunk_kernel<S, C, BC, CM, false><<<nchunks, 256, 0, st>>>(V);
+}
+
+template <class S, class C, int BC>
+void launch_group_bc(const BatchGroupView<S, C>& V, uint32_t nchunks, int cm, bool obs, cudaStream_t st) {
+    switch (cm) {
+        case CM_STRICT: launch_group_bc_cm<S, C, BC, CM_STRICT>(V, nchunks, obs, st); break;
+        case CM_STRICT_GENERIC: launch_group_bc_cm<S, C, BC, CM_STRICT_GENERIC>(V, nchunks, obs, st); break;
+        case CM_FAST:
+            if constexpr (sizeof(C) == 4) launch_group_bc_cm<S, C, BC, CM_FAST>(V, nchunks, obs, st);
+            break;
+        default:
+            if constexpr (sizeof(C) == 4) launch_group_bc_cm<S, C, BC, CM_FAST_GENERIC>(V, nchunks, obs, st);
+            break;
+    }
+}
+
+// One group of a batch step (batch.cuh, grouped form): nchunks blocks over
+// the group's chunk table.
+template <class S, class C>
+int launch_batch_group(const void* desc, const void* chunks, uint32_t nchunks, uint32_t chunk_warps, int parity,
+                       int bcase, int cm, bool obs, cudaStream_t st) {
+    if (nchunks == 0) return BGK_OK;
+    BatchGroupView<S, C> V;
+    V.desc = static_cast<const SweepArgs<S, C>*>(desc);
+    V.chunks = static_cast<const uint2*>(chunks);
+    V.parity = parity;
+    V.chunk_warps = chunk_warps;
+    switch (bcase) {
+        case BC_DRIVEN: launch_group_bc<S, C, BC_DRIVEN>(V, nchunks, cm, obs, st); break;
+        case BC_PERIODIC: launch_group_bc<S, C, BC_PERIODIC>(V, nchunks, cm, obs, st); break;
+        case BC_CHANNEL: launch_group_bc<S, C, BC_CHANNEL>(V, nchunks, cm, obs, st); break;
+        case BC_INFLOW: launch_group_bc<S, C, BC_INFLOW>(V, nchunks, cm, obs, st); break;
+        default: return set_error(BGK_ERR_ARG, "batch members need a boundary case");
+    }
+    return check_launch("batch_chunk_kernel");
+}
+
 template <class S, class C>
 int launch_outflow(const bgk_sweep_params* p, void* const* a, cudaStream_t st) {
     SweepArgs<S, C> A = sweep_args<S, C>(p, a, a);
@@ -490,6 +531,8 @@ int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n,
                                           void*, uint32_t*);                                       \
     template int launch_batch<S, C>(const void*, const uint32_t*, int, uint32_t, unsigned*, int,   \
                                     int, int, cudaStream_t);                                       \
+    template int launch_batch_group<S, C>(const void*, const void*, uint32_t, uint32_t, int, int,   \
+                                          int, bool, cudaStream_t);                                \
     }
 #define BGK_INSTANTIATE_MISC(S, C)                                                                 \
     namespace bgk {                                                                                \

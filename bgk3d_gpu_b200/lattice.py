@@ -334,8 +334,11 @@ class Lattice:
 
 
 class Batch:
-    """Many Lattice objects (AB pattern, one storage kind) advanced together by
-    one persistent launch per step over a device tile queue (bgk_batch_*)."""
+    """Many Lattice objects (AB pattern, one storage kind) advanced together
+    (bgk_batch_*): by default one launch per group of members that share a
+    boundary case, collision mode and obstacle logic, blocks taking chunks of
+    one member's warp segments; or one persistent launch over a device tile
+    queue (set_config)."""
 
     def __init__(self, lattices):
         self.L = lib()
@@ -380,7 +383,32 @@ class Batch:
         return a.value, b.value
 
     def set_config(self, tiles_per_grab: int, blocks_per_sm: int) -> None:
+        """Select the tile-queue form with these parameters."""
+        check(self.L.bgk_batch_set_chunk(self.h, 0), "set_chunk")
         check(self.L.bgk_batch_set_config(self.h, tiles_per_grab, blocks_per_sm), "set_config")
+
+    @property
+    def chunk(self) -> int:
+        w = ctypes.c_int()
+        check(self.L.bgk_batch_get_chunk(self.h, ctypes.byref(w)), "get_chunk")
+        return w.value
+
+    def set_chunk(self, warps_per_chunk: int) -> None:
+        """Select the grouped form with this many warp segments per chunk (0: tile queue)."""
+        check(self.L.bgk_batch_set_chunk(self.h, int(warps_per_chunk)), "set_chunk")
+
+    @property
+    def groups(self) -> int:
+        """Launches per step of the grouped form (groups + solo members)."""
+        return int(self.L.bgk_batch_groups(self.h))
+
+    @property
+    def solo(self) -> int:
+        return int(self.L.bgk_batch_get_solo(self.h))
+
+    def set_solo(self, min_nodes: int) -> None:
+        """Members of min_nodes nodes or more step with their own launch (0: none)."""
+        check(self.L.bgk_batch_set_solo(self.h, int(min_nodes)), "set_solo")
 
     @property
     def nodes(self) -> int:

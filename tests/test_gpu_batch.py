@@ -70,14 +70,31 @@ def test_batch_tune_and_configs():
     from bgk3d_gpu_b200.lattice import Batch
     lats, refs, _ = _make()
     batch = Batch(lats)
+    # kernel variants: periodic (2 members), channel (generic collision),
+    # driven, inflow with obstacle
+    assert batch.groups == 4
     used = batch.tune(2)
     assert used > 0 and used % 2 == 0
     sub, bpsm = batch.config
     assert 1 <= sub <= 16 and 0 <= bpsm <= 8
+    assert batch.chunk in (0, 8, 16, 32, 64, 128)
     for cfg in [(1, 2), (4, 3), (16, 1)]:
         batch.set_config(*cfg)
+        assert batch.chunk == 0
         batch.step(3)
         used += 3
+    for warps in (8, 56, 1024):
+        batch.set_chunk(warps)
+        assert batch.chunk == warps
+        batch.step(3)
+        used += 3
+    # members of 8192 nodes or more (32^3, 48x20x16, 40x24x20, 64x64x8) solo
+    batch.set_solo(8192)
+    assert batch.groups == 5
+    batch.step(3)
+    batch.step(33)
+    used += 36
+    batch.set_solo(0)
     for a, b in zip(lats, refs):
         b.step(used)
         assert np.array_equal(a.download(), b.download())
@@ -111,13 +128,19 @@ def test_batch_resync_after_reload():
     batch.close()
 
 
-@pytest.mark.parametrize("cfg", [(2, 4), (1, 0)])
+@pytest.mark.parametrize("cfg", [(2, 4), (1, 0), 16, 32, "solo"])
 def test_batch_odd_start_then_graph(cfg):
-    """An odd step count first, then a graph run starting from odd parity."""
+    """An odd step count first, then a graph run starting from odd parity
+    (tile-queue forms and grouped form)."""
     from bgk3d_gpu_b200.lattice import Batch
     lats, refs, _ = _make()
     batch = Batch(lats)
-    batch.set_config(*cfg)
+    if isinstance(cfg, tuple):
+        batch.set_config(*cfg)
+    elif cfg == "solo":
+        batch.set_solo(10000)   # every member but the 17x9x11 cavity steps solo
+    else:
+        batch.set_chunk(cfg)
     batch.step(3)
     batch.step(37)
     for a, b in zip(lats, refs):
