@@ -106,6 +106,8 @@ def lib() -> ctypes.CDLL:
     L.bgk_set_pair_kernels.restype = c_int
     L.bgk_abi_struct_size.argtypes = [c_int]
     L.bgk_abi_struct_size.restype = c_size_t
+    L.bgk_abi_field_offset.argtypes = [c_int, c_int]
+    L.bgk_abi_field_offset.restype = c_longlong
     _bind_lattice(L)
     _lib = L
     return L

@@ -2,6 +2,7 @@
 // shapes around the kernels of sweep_ab.cuh and reduce.cuh.
 #include <cuda_runtime.h>
 #include <cstdio>
+#include <cstddef>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -261,6 +262,34 @@ int bgk_dropin_finalize(const double* partials, long long nparts, double* out_de
 const char* bgk_last_error(void) { return g_last_error.c_str(); }
 
 const char* bgk_version(void) { return "bgk3d_b200 0.1 (sm_100a)"; }
+
+long long bgk_abi_field_offset(int which, int field) {
+#define BGK_OFF(T, f) (long long)offsetof(T, f)
+    static const long long sweep[] = {
+        BGK_OFF(bgk_sweep_params, kind), BGK_OFF(bgk_sweep_params, bcase), BGK_OFF(bgk_sweep_params, l),
+        BGK_OFF(bgk_sweep_params, m), BGK_OFF(bgk_sweep_params, n), BGK_OFF(bgk_sweep_params, nx),
+        BGK_OFF(bgk_sweep_params, ny), BGK_OFF(bgk_sweep_params, omega), BGK_OFF(bgk_sweep_params, cte0),
+        BGK_OFF(bgk_sweep_params, cte1), BGK_OFF(bgk_sweep_params, p0), BGK_OFF(bgk_sweep_params, p1),
+        BGK_OFF(bgk_sweep_params, p2), BGK_OFF(bgk_sweep_params, rf), BGK_OFF(bgk_sweep_params, qf),
+        BGK_OFF(bgk_sweep_params, tre), BGK_OFF(bgk_sweep_params, force_mode), BGK_OFF(bgk_sweep_params, fx),
+        BGK_OFF(bgk_sweep_params, fy), BGK_OFF(bgk_sweep_params, fz), BGK_OFF(bgk_sweep_params, lid_force),
+        BGK_OFF(bgk_sweep_params, u_inflow), BGK_OFF(bgk_sweep_params, inflow_cte1),
+        BGK_OFF(bgk_sweep_params, scale), BGK_OFF(bgk_sweep_params, obs), BGK_OFF(bgk_sweep_params, obs_nx),
+        BGK_OFF(bgk_sweep_params, obs_ny), BGK_OFF(bgk_sweep_params, imin), BGK_OFF(bgk_sweep_params, imax),
+        BGK_OFF(bgk_sweep_params, jmin), BGK_OFF(bgk_sweep_params, jmax), BGK_OFF(bgk_sweep_params, kmin),
+        BGK_OFF(bgk_sweep_params, kmax), BGK_OFF(bgk_sweep_params, fast), BGK_OFF(bgk_sweep_params, zhalo)};
+    static const long long desc[] = {
+        BGK_OFF(bgk_lattice_desc, kind), BGK_OFF(bgk_lattice_desc, bcase), BGK_OFF(bgk_lattice_desc, pattern),
+        BGK_OFF(bgk_lattice_desc, l), BGK_OFF(bgk_lattice_desc, m), BGK_OFF(bgk_lattice_desc, n),
+        BGK_OFF(bgk_lattice_desc, omega), BGK_OFF(bgk_lattice_desc, force_mode), BGK_OFF(bgk_lattice_desc, fx),
+        BGK_OFF(bgk_lattice_desc, fy), BGK_OFF(bgk_lattice_desc, fz), BGK_OFF(bgk_lattice_desc, lid_force),
+        BGK_OFF(bgk_lattice_desc, u_inflow), BGK_OFF(bgk_lattice_desc, scale), BGK_OFF(bgk_lattice_desc, fast)};
+#undef BGK_OFF
+    if (field < 0) return -1;
+    if (which == 0) return field < (int)(sizeof sweep / sizeof *sweep) ? sweep[field] : -1;
+    if (which == 1) return field < (int)(sizeof desc / sizeof *desc) ? desc[field] : -1;
+    return -1;
+}
 
 size_t bgk_abi_struct_size(int which) {
     switch (which) {

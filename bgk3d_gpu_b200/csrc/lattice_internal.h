@@ -12,6 +12,7 @@ struct bgk_lattice {
     bgk_sweep_params p;          // sweep parameters (kind, case, constants, layout, obstacle)
     int es;                      // bytes per stored value
     long long nx, ny, nz, origin, plane;   // elements
+    long long shift = 0;                   // elements before the first plane's origin (128-byte row starts)
     char* base = nullptr;
     size_t bytes = 0;
     std::vector<void*> planes;   // plane pointers at element (0,0,0)

@@ -211,6 +211,10 @@ const char* bgk_version(void);
    another language (Fortran bind(C) types, Python ctypes) checks its mirror
    against it.  No counterpart in the reference. */
 size_t bgk_abi_struct_size(int which);
+/* Byte offset of field number `field` (declaration order, from 0) of the
+   same structs, or -1 past the last field: a mirror checks every field's
+   place, not only the total size.  No counterpart in the reference. */
+long long bgk_abi_field_offset(int which, int field);
 
 /* Two-node sweeps for the 16-bit kinds (FP16 / BF16 storage, FP32 compute)
    without fused moments (warps next to an obstacle advance their nodes one

@@ -91,3 +91,19 @@ def test_struct_mirrors_match_the_library():
     assert L.bgk_abi_struct_size(0) == ctypes.sizeof(SweepParams)
     assert L.bgk_abi_struct_size(1) == ctypes.sizeof(LatticeDesc)
     assert L.bgk_abi_struct_size(7) == 0
+
+
+def test_struct_mirror_fields_sit_where_the_library_has_them():
+    """Every field of the ctypes mirrors, in declaration order, at the byte
+    offset the library was compiled with: two swapped fields of equal total
+    size, or a field moved into a padding hole, would pass the size check
+    and shift the values the kernels read."""
+    from bgk3d_gpu_b200._lib import SweepParams, lib
+    from bgk3d_gpu_b200._lattice_abi import LatticeDesc
+    L = lib()
+    for which, mirror in ((0, SweepParams), (1, LatticeDesc)):
+        fields = [getattr(mirror, name) for name, _ in mirror._fields_]
+        for idx, f in enumerate(fields):
+            assert L.bgk_abi_field_offset(which, idx) == f.offset, (mirror.__name__, mirror._fields_[idx][0])
+        assert L.bgk_abi_field_offset(which, len(fields)) == -1
+    assert L.bgk_abi_field_offset(5, 0) == -1

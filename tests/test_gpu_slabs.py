@@ -2,14 +2,16 @@
 this process, faces exchanged by device copies between the steps) gives,
 after every step, the state of the undivided lattice bit for bit, for the
 periodic, driven-cavity and channel cases, every storage kind and both
-collision modes (the 16-bit kinds through the pair sweep); the moments add
-up; unsupported combinations are refused."""
+collision modes (the 16-bit kinds through the pair sweep), and -- in the
+reference's operation order -- the CPU oracle's state of the whole lattice
+bit for bit; the moments add up; unsupported combinations are refused."""
 import zlib
 
 import numpy as np
 import pytest
 
-from _cases import BCASE, CASE_PARAMS, OMEGA, SCALE, interior, random_state
+from _cases import (BCASE, CASE_PARAMS, OMEGA, SCALE, assert_fluid_equal, interior, oracle_step_kwargs,
+                    random_state)
 
 pytestmark = pytest.mark.gpu
 
@@ -38,6 +40,11 @@ def test_slabs_equal_the_undivided_lattice(kind, case, parts):
         slabs = [Slab(r, parts, l, m, n, bcase=BCASE[case], **kw) for r in range(parts)]
         for s in slabs:
             s.upload_global(st)
+        orc = None
+        if not fast:   # the fused collision is not the reference's operation order
+            from oracle.oracle import OracleLattice
+            orc = OracleLattice(l, m, n, kind, scale=SCALE[kind])
+            orc.set_state(st)
         tr = LocalTransport()
         tr.exchange_all(slabs)
         for step in range(5):
@@ -49,6 +56,10 @@ def test_slabs_equal_the_undivided_lattice(kind, case, parts):
             want = interior(whole.download(), l, m, n)
             bad = np.argwhere(got != want)
             assert len(bad) == 0, (kind, case, parts, fast, step, len(bad), bad[:5].tolist())
+            if orc is not None:
+                orc.step(BCASE[case], OMEGA, 1, **oracle_step_kwargs(case))
+                assert_fluid_equal(got, orc.interior(), np.ones((n, m, l), bool),
+                                   f"slabs vs oracle kind={kind} case={case} parts={parts} step={step}")
         mw = whole.moments()
         ms = sum(s.lat.moments() for s in slabs)
         assert np.allclose(ms, mw, rtol=1e-12, atol=1e-12), (ms, mw)
