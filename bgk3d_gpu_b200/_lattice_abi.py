@@ -62,6 +62,8 @@ def bind(L) -> None:
     L.bgk_lattice_create.restype = c_int
     L.bgk_lattice_destroy.argtypes = [c_void_p]
     L.bgk_lattice_destroy.restype = c_int
+    L.bgk_lattice_destroy_async.argtypes = [c_void_p, c_void_p]
+    L.bgk_lattice_destroy_async.restype = c_int
     L.bgk_lattice_set_obstacle.argtypes = [c_void_p, c_void_p]
     L.bgk_lattice_set_obstacle.restype = c_int
     L.bgk_lattice_save.argtypes = [c_void_p, ctypes.c_char_p, c_int, c_int, c_void_p]

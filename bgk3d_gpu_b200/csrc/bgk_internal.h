@@ -70,6 +70,9 @@ int finalize_moments(const double* partials, long long nparts, double* out, cuda
 // the device, as cudaFree does, and returns the block to the pool.
 int dev_alloc(void** p, size_t bytes, bool zero, const char* what);
 void dev_free(void* p);
+// Return the block to the pool ordered after the work queued on st (no
+// device-wide wait): every use of p must be on st or ordered before it.
+void dev_free_async(void* p, cudaStream_t st);
 // Private non-blocking stream for set-up kernels and copies.
 cudaStream_t setup_stream();
 // The launches of the turbulence diagnostics (TKE, dissipation, mean

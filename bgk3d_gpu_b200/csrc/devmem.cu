@@ -91,6 +91,11 @@ void dev_free(void* p) {
     }
 }
 
+void dev_free_async(void* p, cudaStream_t st) {
+    if (!p) return;
+    cudaFreeAsync(p, st);               // after the work queued on st
+}
+
 cudaStream_t setup_stream() {
     DevicePool* P = nullptr;
     if (current_pool(&P)) return nullptr;

@@ -344,6 +344,22 @@ int bgk_set_tma_kernels(int enable) {
     return prev;
 }
 
+int bgk_lattice_destroy_async(bgk_lattice* L, void* stream) {
+    if (!L) return BGK_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    // an executable graph or a stream still in flight is released when its
+    // work completes
+    drop_graph(L);
+    if (L->cap_stream) cudaStreamDestroy(L->cap_stream);
+    dev_free_async(L->base, st);
+    dev_free_async(L->obs_dev, st);
+    dev_free_async(L->ws, st);
+    dev_free_async(L->mom, st);
+    dev_free_async(L->err, st);
+    delete L;
+    return BGK_OK;
+}
+
 int bgk_lattice_destroy(bgk_lattice* L) {
     if (!L) return BGK_OK;
     drop_graph(L);

@@ -194,9 +194,14 @@ class Lattice:
         self.h = h
         self._out = torch.zeros(8, dtype=torch.float64, device=self.device)
 
-    def close(self):
+    def close(self, stream=None):
+        """Free the lattice; with a torch stream, stream-ordered after the work
+        queued on it (every use of the lattice must be on that stream)."""
         if getattr(self, "h", None):
-            self.L.bgk_lattice_destroy(self.h)
+            if stream is None:
+                self.L.bgk_lattice_destroy(self.h)
+            else:
+                self.L.bgk_lattice_destroy_async(self.h, stream.cuda_stream)
             self.h = None
 
     def __del__(self):

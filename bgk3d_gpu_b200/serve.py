@@ -15,6 +15,12 @@ the library's pool, which keeps freed blocks for the next request
 leaves as soon as its steps are done; its result is the FP64 moments (and,
 for the sphere, drag/lift) of its final state.
 
+With the default small-lattice policy ("streams") the continuous and
+shared modes run without rounds: every solve steps on its own stream with at
+most two chunks of steps in flight, and the host retires, admits and tops up
+solves as per-solve events complete (_run_async), so neither admission nor
+retirement waits for the whole device.  `rounds=True` keeps the round loop.
+
 Round policies (`mode`):
   continuous  shortest remaining work first with a saturation floor: the
               solves with the least remaining work (steps x nodes) are taken
@@ -129,7 +135,7 @@ class _Active:
 
 class Server:
     def __init__(self, budget_bytes: float = 150e9, max_chunk: int = 200, floor_nodes: float = 8e6,
-                 alone_nodes: float = 2e6, small: str = "streams", nstreams: int = 8):
+                 alone_nodes: float = 2e6, small: str = "streams", nstreams: int = 8, rounds: bool = False):
         free, _ = torch.cuda.mem_get_info()
         self.budget = min(budget_bytes, free * 0.92)
         self.max_chunk = max_chunk
@@ -147,6 +153,9 @@ class Server:
             raise ValueError(f"unknown small-lattice policy {small!r}")
         self.small = small
         self.streams = [torch.cuda.Stream() for _ in range(nstreams)] if small == "streams" else []
+        # rounds=True keeps the round-based loop (device-wide synchronisation
+        # after every round) for the streams policy too
+        self.rounds = rounds
 
     def select(self, active, mode: str):
         """The solves stepped this round (see the module docstring)."""
@@ -164,6 +173,8 @@ class Server:
         """Serve the trace; returns (per-request records, summary)."""
         if mode not in ("continuous", "shared", "fifo", "plain"):
             raise ValueError(f"unknown mode {mode!r}")
+        if mode in ("continuous", "shared") and self.small == "streams" and not self.rounds:
+            return self._run_async(trace, mode, keep_states)
         one_at_a_time = mode in ("fifo", "plain")
         pending = sorted(trace, key=lambda r: r.arrival)
         active: list[_Active] = []
@@ -269,6 +280,118 @@ class Server:
         return done, summary
 
 
+    def _run_async(self, trace, mode: str, keep_states: bool):
+        """continuous / shared without rounds: every admitted solve steps on
+        its own stream (from a pool) with up to two chunks of at most
+        max_chunk steps in flight; the host watches per-solve events,
+        retires a solve as soon as its last chunk completes (its moments on
+        its own stream, its memory freed stream-ordered), admits arrivals
+        between chunks and tops the selected solves up again, so the GPU queue
+        never drains between chunks and nothing waits for the whole device.
+        The continuous policy selects by remaining unscheduled work (steps not
+        yet queued x nodes) with the same saturation floor."""
+        from collections import deque
+        pending = sorted(trace, key=lambda r: r.arrival)
+        active: list[_Active] = []
+        done = []
+        used = 0
+        lups = 0
+        issued = 0
+        set_retained_bytes(int(self.budget))
+        nstreams = max(len(self.streams), 1)
+        t0 = time.perf_counter()
+        t_admit = t_wait = 0.0
+        next_stream = 0
+
+        def admit(now):
+            nonlocal used, t_admit, next_stream
+            ta = time.perf_counter()
+            while pending and pending[0].arrival <= now:
+                need = lattice_bytes(pending[0])
+                if need > self.budget:
+                    raise RuntimeError(f"request {pending[0].rid} needs {need} bytes, more than the budget")
+                if used + need > self.budget:
+                    break
+                a = _Active(pending.pop(0), now)
+                a.stream = self.streams[next_stream % nstreams]
+                next_stream += 1
+                # the set-up (creation, initial state) ran on the current stream
+                a.stream.wait_stream(torch.cuda.current_stream())
+                a.left = a.remaining            # steps not yet queued
+                a.inflight = deque()
+                active.append(a)
+                used += a.bytes
+            t_admit += time.perf_counter() - ta
+
+        class _Sched:
+            def __init__(self, a):
+                self.a, self.req, self.nodes, self.remaining = a, a.req, a.nodes, a.left
+
+        try:
+            while pending or active:
+                admit(time.perf_counter() - t0)
+                if not active:
+                    if pending:
+                        time.sleep(max(0.0, min(0.01, pending[0].arrival - (time.perf_counter() - t0))))
+                    continue
+                # top up the selected solves (selection by unscheduled work)
+                cand = [_Sched(a) for a in active if a.left > 0]
+                for sch in (self.select(cand, mode) if cand else []):
+                    a = sch.a
+                    while len(a.inflight) < 2 and a.left > 0:
+                        chunk = min(self.max_chunk, a.left)
+                        with torch.cuda.stream(a.stream):
+                            a.lat.step(chunk)
+                            ev = torch.cuda.Event()
+                            ev.record(a.stream)
+                        a.inflight.append((ev, chunk))
+                        a.left -= chunk
+                        issued += 1
+                # completed chunks; wait briefly when nothing has completed
+                tw = time.perf_counter()
+                progressed = False
+                while not progressed:
+                    for a in active:
+                        while a.inflight and a.inflight[0][0].query():
+                            _, c = a.inflight.popleft()
+                            a.remaining -= c
+                            lups += c * a.nodes
+                            progressed = True
+                    if not progressed:
+                        if pending and pending[0].arrival <= time.perf_counter() - t0:
+                            break            # admit the arrival, then top up again
+                        if not any(a.inflight for a in active):
+                            break
+                        time.sleep(2e-4)
+                t_wait += time.perf_counter() - tw
+                finished = [a for a in active if a.remaining == 0]
+                if finished:
+                    t_done = time.perf_counter() - t0
+                    for a in finished:
+                        with torch.cuda.stream(a.stream):
+                            res = a.result()
+                            rec = {"rid": a.req.rid, "case": a.req.case, "side": a.req.side, "steps": a.req.steps,
+                                   "kind": a.req.kind, "arrival": a.req.arrival, "admitted": a.t_admit,
+                                   "completed": t_done, "latency": t_done - a.req.arrival, **res}
+                            if keep_states:
+                                rec["state"] = a.lat.download()
+                        done.append(rec)
+                        active.remove(a)
+                        used -= a.bytes
+                        a.lat.close(stream=a.stream)
+        finally:
+            torch.cuda.synchronize()
+            set_retained_bytes(0)
+        wall = time.perf_counter() - t0
+        lat = np.array([d["latency"] for d in done])
+        summary = {"mode": mode, "requests": len(done), "wall_s": wall, "rounds": issued,
+                   "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                   "mean_latency_s": float(lat.mean()), "aggregate_glups": lups / wall / 1e9,
+                   "solves_per_s": len(done) / wall, "budget_gb": self.budget / 1e9,
+                   "host_admission_s": t_admit, "gpu_wait_s": t_wait, "scheduling": "per-solve streams and events"}
+        return done, summary
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=60)
@@ -280,6 +403,8 @@ def main(argv=None):
     ap.add_argument("--alone-nodes", type=float, default=2e6)
     ap.add_argument("--small", default="streams", choices=["batch", "streams"],
                     help="lattices below --alone-nodes: one tile-queue launch per kind, or each on a side stream")
+    ap.add_argument("--rounds", action="store_true",
+                    help="streams policy: rounds ended by a device-wide synchronisation instead of per-solve events")
     ap.add_argument("--fast", action="store_true",
                     help="solve every request with the fused-multiply-add collision (FP16 requests then take "
                          "the two-node sweep; L2 velocity error unchanged at the FP16 storage level)")
@@ -295,7 +420,7 @@ def main(argv=None):
                      "total_lups": sum(r.side ** 3 * (2 if r.case == "sphere" else 1) * r.steps for r in trace)}}
     for mode in args.modes.split(","):
         _, summary = Server(args.budget_gb * 1e9, floor_nodes=args.floor_nodes, alone_nodes=args.alone_nodes,
-                            small=args.small).run(trace, mode=mode)
+                            small=args.small, rounds=args.rounds).run(trace, mode=mode)
         out[mode] = summary
         print(json.dumps({mode: summary}), flush=True)
     if "continuous" in out and "fifo" in out:

@@ -54,6 +54,12 @@ size_t bgk_lattice_device_bytes(const bgk_lattice_desc* d);
    like cudaFree. */
 int bgk_lattice_create(const bgk_lattice_desc* d, bgk_lattice** out);
 int bgk_lattice_destroy(bgk_lattice* lat);
+/* Destroy without waiting for the device: the lattice's memory goes back to
+   the pool ordered after the work queued on `stream`.  Every launch and copy
+   that used the lattice must be on that stream or ordered before the call
+   (a server that steps each solve on its own stream retires it this way
+   while the other solves keep running).  No counterpart in the reference. */
+int bgk_lattice_destroy_async(bgk_lattice* lat, void* stream);
 
 /* Bytes of freed lattice memory the current device's pool keeps for reuse
    (default 0: freed memory goes back to the device at once).  A server that

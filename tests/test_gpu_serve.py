@@ -39,17 +39,21 @@ def _alone(req):
                                                    ("shared", 0, False, "batch"),
                                                    ("continuous", 3e4, True, "batch"),
                                                    ("continuous", 3e4, False, "streams"),
-                                                   ("shared", 0, True, "streams")])
+                                                   ("shared", 0, True, "streams"),
+                                                   ("continuous", 3e4, False, "rounds")])
 def test_results_identical_alone_and_in_the_mix(mode, floor, fast, small):
     """floor 3e4 nodes makes the shortest-work-first policy step only a few
     solves per round, so batches change membership between rounds.  With the
     fused collision the FP16 requests step alone through the two-node sweep
     and in the mix through the batched one-node sweep: still bit-identical.
-    With small="streams" the small solves step side by side on their own
-    streams instead of through the tile queue."""
+    With small="streams" every solve steps on its own stream with per-solve
+    events (no rounds), "rounds" is the same policy in device-synchronised
+    rounds."""
     from bgk3d_gpu_b200.serve import Server
     trace = _trace(fast)
-    done, summary = Server(budget_bytes=20e9, max_chunk=25, floor_nodes=floor, small=small).run(
+    rounds = small == "rounds"
+    done, summary = Server(budget_bytes=20e9, max_chunk=25, floor_nodes=floor,
+                           small="streams" if rounds else small, rounds=rounds).run(
         trace, mode=mode, keep_states=True)
     assert summary["requests"] == len(trace)
     assert summary["rounds"] > len(trace)       # solves shared rounds
