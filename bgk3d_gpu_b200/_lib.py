@@ -102,6 +102,8 @@ def lib() -> ctypes.CDLL:
     L.bgk_last_error.restype = c_char_p
     L.bgk_version.argtypes = []
     L.bgk_version.restype = c_char_p
+    L.bgk_set_obstacle_split.argtypes = [c_int]
+    L.bgk_set_obstacle_split.restype = c_int
     L.bgk_set_pair_kernels.argtypes = [c_int]
     L.bgk_set_pair_kernels.restype = c_int
     L.bgk_abi_struct_size.argtypes = [c_int]

@@ -238,7 +238,8 @@ int member_step(bgk_batch* B, int idx, int par, cudaStream_t st) {
     member_arrays(B, (size_t)idx, par, a);
     member_arrays(B, (size_t)idx, par ^ 1, b);
     b[18] = a[18];
-    return sweep_launch(&B->lats[idx]->p, a, b, st);
+    int halo = 0;   // pre-pass, and the next outflow plane written like the member's own step
+    return sweep_launch_mom(&B->lats[idx]->p, a, b, nullptr, st, &halo);
 }
 
 // One step of a work item (solo member idx >= 0, or group -1 - idx).
@@ -303,6 +304,7 @@ void sync_members(bgk_batch* B, long long nsteps) {
     for (size_t i = 0; i < B->lats.size(); ++i) {
         B->lats[i]->steps += nsteps;
         B->expect[i] = B->lats[i]->steps;
+        if (nsteps) B->lats[i]->outflow_fresh = false;   // batched steps do not write the next outflow plane
     }
 }
 

@@ -124,8 +124,8 @@ int bgk::sweep_launch(const bgk_sweep_params* p, void* const* a, void* const* b,
 }
 
 int bgk::sweep_launch_mom(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom,
-                          cudaStream_t st) {
-    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, mom, st)));
+                          cudaStream_t st, int* halo) {
+    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, mom, st, halo)));
 }
 
 int bgk::dissipation_launch(const bgk_sweep_params* p, void* const* a, double nu, double* out, double* ws,
@@ -146,6 +146,12 @@ int bgk::draglift_launch(const bgk_sweep_params* p, void* const* a, int is, int 
 }
 
 extern "C" {
+
+int bgk_set_obstacle_split(int enable) {
+    const int prev = g_obstacle_split ? 1 : 0;
+    g_obstacle_split = enable != 0;
+    return prev;
+}
 
 int bgk_set_pair_kernels(int enable) {
     const int prev = g_pair_kernels ? 1 : 0;

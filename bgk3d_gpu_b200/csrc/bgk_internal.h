@@ -31,6 +31,11 @@ inline SegPlan seg_plan(int l, int m, int n, long long nx, long long align_base,
 // Off by default: bit-exact, 280 instead of 408 instructions per node for
 // FP16, but measured at half the one-node kernel's rate on 256^3 (B200).
 inline bool g_tma_kernels = false;
+// One-node AB sweep with an obstacle as two launches (the obstacle-free
+// variant outside the obstacle's grown box, sweep_box_kernel inside it):
+// bgk_set_obstacle_split(1).  Off by default: measured 4-7 % slower than one
+// launch with the obstacle logic (FP32 sphere case at 256^3, B200).
+inline bool g_obstacle_split = false;
 // Two-node sweep for the 16-bit kinds (sweep_ab2_kernel): on by default;
 // bgk_set_pair_kernels(0) selects the one-node sweep (tests compare both).
 inline bool g_pair_kernels = true;
@@ -50,9 +55,11 @@ int moments_launch(const struct bgk_sweep_params* p, void* const* a, double* out
                    cudaStream_t st);
 // The fused sweep launch(es) without argument validation.
 int sweep_launch(const struct bgk_sweep_params* p, void* const* a, void* const* b, cudaStream_t st);
-// Same, with the per-block FP64 moments of the new state written to mom.
+// Same, with the per-block FP64 moments of the new state written to mom;
+// halo (inflow, nullable): in, a's outflow plane is fresh (no pre-pass); out,
+// the launch wrote the next state's outflow plane into b.
 int sweep_launch_mom(const struct bgk_sweep_params* p, void* const* a, void* const* b, double* mom,
-                     cudaStream_t st);
+                     cudaStream_t st, int* halo = nullptr);
 // Blocks of a sweep launch that also produces moments: a fixed grid (20
 // blocks per SM of the current device, fewer for small lattices) strides over
 // the step's warps.  The partial sums, and so the last bits of the moments,

@@ -65,6 +65,15 @@ FastConst<C> fast_const(const bgk_sweep_params* p, double sc) {
     return f;
 }
 
+// A compute value rounded to storage kind S on the host, as Conv<S, C>::pack
+// rounds it on the device (round to nearest even).
+template <class S, class C> inline S host_pack(C v);
+template <> inline double host_pack<double, double>(double v) { return v; }
+template <> inline float host_pack<float, float>(float v) { return v; }
+template <> inline float host_pack<float, double>(double v) { return (float)v; }
+template <> inline __half host_pack<__half, float>(float v) { return __float2half_rn(v); }
+template <> inline __nv_bfloat16 host_pack<__nv_bfloat16, float>(float v) { return __float2bfloat16_rn(v); }
+
 template <class S, class C>
 SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* const* b) {
     SweepArgs<S, C> A;
@@ -80,6 +89,10 @@ SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* cons
     A.lid_force = (C)p->lid_force * (C)sc;
     A.u_inflow = (C)p->u_inflow;
     A.inflow_cte1 = (C)p->inflow_cte1;
+    // the inflow face's five equilibria are constants of the lattice: the
+    // same operations in the same type as inflow_eq runs on the device
+    // (separate IEEE roundings on both sides), rounded to storage once here
+    for (int d = 0; d < 5; ++d) A.inflow_s[d] = host_pack<S, C>(inflow_eq<C>(d, A.u_inflow, A.inflow_cte1, A.col));
     A.scale = (p->kind == K_F16 || p->kind == K_BF16) ? p->scale : 1.0f;
     A.inv_scale = 1.0f / A.scale;
     const bool has_obs = p->obs && p->imin <= p->imax && p->jmin <= p->jmax && p->kmin <= p->kmax;
@@ -92,6 +105,7 @@ SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* cons
     A.generic = !(p->cte1 == 1.0 && p->cte0 == 0.0 && p->fx == 0.0 && p->fy == 0.0 && p->fz == 0.0);
     A.fast = (p->fast != 0 && sizeof(C) == 4) ? 1 : 0;
     A.zhalo = p->zhalo & 3;
+    A.outflow_next = 0;
     return A;
 }
 

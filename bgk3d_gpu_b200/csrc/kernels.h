@@ -9,7 +9,8 @@
 
 namespace bgk {
 template <class S, class C>
-int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st);
+int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st,
+                 int* halo = nullptr);
 template <class S, class C>
 int launch_sweep_tma(const bgk_sweep_params* p, void* const* a, void* const* b, const void* tmap, const int* pa,
                      int* err, cudaStream_t st);

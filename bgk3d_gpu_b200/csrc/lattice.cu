@@ -87,8 +87,11 @@ int one_step(bgk_lattice* L, cudaStream_t st, double* mom = nullptr) {
         const bool has_obs = L->p.obs && L->p.imin <= L->p.imax;
         if (!mom && L->tma_ok && g_tma_kernels && !has_obs && !L->p.zhalo) {
             if (int e = tma_step(L, st)) return e;
-        } else if (int e = sweep_launch_mom(&L->p, L->a, L->b, mom, st)) {
-            return e;
+            L->outflow_fresh = false;
+        } else {
+            int halo = L->outflow_fresh ? 1 : 0;
+            if (int e = sweep_launch_mom(&L->p, L->a, L->b, mom, st, &halo)) return e;
+            L->outflow_fresh = halo != 0;
         }
         for (int d = 0; d < 18; ++d) std::swap(L->a[d], L->b[d]);
     }
@@ -106,12 +109,18 @@ int build_graph(bgk_lattice* L) {
     const long long saved = L->steps;
     void* a0[19]; void* b0[19];
     std::memcpy(a0, L->a, sizeof a0); std::memcpy(b0, L->b, sizeof b0);
+    const bool fresh0 = L->outflow_fresh;
+    // a replay may follow a load: the graph's first step recomputes the
+    // outflow plane (inflow case), its later steps take it from the step before
+    L->outflow_fresh = false;
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamBeginCapture(L->cap_stream, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) { L->outflow_fresh = fresh0; return set_error(BGK_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e)); }
     int rc = BGK_OK;
     for (int s = 0; s < kGraphSteps && rc == BGK_OK; ++s) rc = one_step(L, L->cap_stream);
     e = cudaStreamEndCapture(L->cap_stream, &g);
+    L->graph_fresh = L->outflow_fresh;
+    L->outflow_fresh = fresh0;
     L->steps = saved;
     std::memcpy(L->a, a0, sizeof a0); std::memcpy(L->b, b0, sizeof b0);
     if (rc != BGK_OK) { if (g) cudaGraphDestroy(g); return rc; }
@@ -234,6 +243,7 @@ void begin_load(bgk_lattice* L, void** out) {
 
 int end_load(bgk_lattice* L, cudaStream_t st) {
     L->steps = 0;
+    L->outflow_fresh = false;
     if (L->desc.pattern == BGK_PATTERN_AA && L->desc.bcase == BC_INFLOW)
         if (int e = aa_prepass(&L->p, L->a, st)) return e;
     return BGK_OK;
@@ -535,6 +545,7 @@ int bgk_lattice_step(bgk_lattice* L, int nsteps, void* stream) {
             if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
             L->steps += L->graph_steps;
             left -= L->graph_steps;
+            L->outflow_fresh = L->graph_fresh;
         }
     }
     while (left-- > 0)

@@ -30,6 +30,11 @@ struct bgk_lattice {
     alignas(64) CUtensorMap tmap; // the allocation as x, y, z, plane (sweep_tma.cuh)
     bool tma_ok = false;         // tmap is valid (AB pattern, driver support)
     int* err = nullptr;          // device flag set by a TMA kernel wait that gave up
+    // inflow, AB: the current a arrays' outflow plane holds the equilibria of
+    // the current state (the last step wrote it), so the next step needs no
+    // pre-pass; graph_fresh: the same after a replay of the step graph
+    bool outflow_fresh = false;
+    bool graph_fresh = false;
 };
 
 // Shared by the lattice's host-transfer paths (lattice.cu, lattice_io.cu).

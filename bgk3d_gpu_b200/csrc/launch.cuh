@@ -59,6 +59,13 @@ template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbLaunch
         sweep_ab_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
     }
 };
+// The obstacle's grown box (sweep_box_kernel, obstacle logic compiled in);
+// instantiated through by_variant with OBS = false only.
+template <class S, class C, int BC, class IDX, int CM, bool OBS> struct BoxLaunch {
+    static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
+        if constexpr (!OBS) sweep_box_kernel<S, C, BC, IDX, CM><<<blocks, 256, 0, st>>>(A);
+    }
+};
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct Ab2Launch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
         if constexpr (sizeof(S) == 2 && sizeof(C) == 4 && !OBS)
@@ -99,15 +106,37 @@ template <class S, class C> int coll_mode(const SweepArgs<S, C>& A) {
     return A.generic + ((sizeof(C) == 4 && A.fast) ? 2 : 0);
 }
 
+// halo (inflow, nullable): on entry nonzero when a's outflow plane already
+// holds the equilibria of a's state at x = l (the previous launch wrote it),
+// so the pre-pass is skipped; on return nonzero when this launch wrote the
+// next state's outflow plane into b (the one-node sweep does, the pair
+// sweeps do not).
 template <class S, class C>
-int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st) {
+int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st,
+                 int* halo) {
     SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
     segment_geometry(A, a[0], true);
     A.mom = mom;
+    const bool fresh = halo && *halo;
+    if (halo) *halo = 0;
+    bool one_node = true;   // the path below is the one-node sweep unless a pair path returns first
+    if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
+        const long long ne = p->nx * p->ny * ((long long)p->n + 2) + 64;
+        const int cm0 = coll_mode(A);
+        if (g_pair_kernels && mom == nullptr && ne < (1LL << 31) &&
+            (pairs_aligned<S>(p, a, b) || (cm_fast(cm0) && A.obs == nullptr)))
+            one_node = false;
+    }
     if (p->bcase == BC_INFLOW) {
-        dim3 blk(128), grd((p->m + 127) / 128, p->n);
-        outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
-        if (int e = check_launch("outflow_halo_kernel")) return e;
+        if (!fresh || !one_node) {
+            dim3 blk(128), grd((p->m + 127) / 128, p->n);
+            outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
+            if (int e = check_launch("outflow_halo_kernel")) return e;
+        }
+        if (halo && one_node) {
+            A.outflow_next = 1;
+            *halo = 1;
+        }
     }
     const long long warps = seg_plan(p->l, p->m, p->n, p->nx, A.align_base, true).warps;
     const long long blocks = (warps + 7) / 8;
@@ -152,6 +181,29 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
             }
             return check_launch("sweep_ab2_kernel");
         }
+    }
+    if (obs && g_obstacle_split && mom == nullptr && nelem < (1LL << 31)) {
+        // the obstacle-free variant over every node outside the obstacle's
+        // grown box, then that box with the obstacle logic: the obstacle's
+        // per-link tests cost every node about 20 % more instructions
+        switch (p->bcase) {
+            case BC_NONE: by_variant<AbLaunch, S, C, BC_NONE>(nelem, cm, false, A, nb, st); break;
+            case BC_DRIVEN: by_variant<AbLaunch, S, C, BC_DRIVEN>(nelem, cm, false, A, nb, st); break;
+            case BC_PERIODIC: by_variant<AbLaunch, S, C, BC_PERIODIC>(nelem, cm, false, A, nb, st); break;
+            case BC_CHANNEL: by_variant<AbLaunch, S, C, BC_CHANNEL>(nelem, cm, false, A, nb, st); break;
+            case BC_INFLOW: by_variant<AbLaunch, S, C, BC_INFLOW>(nelem, cm, false, A, nb, st); break;
+        }
+        if (int e = check_launch("sweep_ab_kernel")) return e;
+        const long long box = (long long)(A.imax - A.imin + 3) * (A.jmax - A.jmin + 3) * (A.kmax - A.kmin + 3);
+        const unsigned nbb = (unsigned)((box + 255) / 256);
+        switch (p->bcase) {
+            case BC_NONE: by_variant<BoxLaunch, S, C, BC_NONE>(nelem, cm, false, A, nbb, st); break;
+            case BC_DRIVEN: by_variant<BoxLaunch, S, C, BC_DRIVEN>(nelem, cm, false, A, nbb, st); break;
+            case BC_PERIODIC: by_variant<BoxLaunch, S, C, BC_PERIODIC>(nelem, cm, false, A, nbb, st); break;
+            case BC_CHANNEL: by_variant<BoxLaunch, S, C, BC_CHANNEL>(nelem, cm, false, A, nbb, st); break;
+            case BC_INFLOW: by_variant<BoxLaunch, S, C, BC_INFLOW>(nelem, cm, false, A, nbb, st); break;
+        }
+        return check_launch("sweep_box_kernel");
     }
     switch (p->bcase) {
         case BC_NONE: by_variant<AbLaunch, S, C, BC_NONE>(nelem, cm, obs, A, nb, st); break;
@@ -400,6 +452,18 @@ template <class S, class C>
 size_t fill_batch_desc(const bgk_sweep_params* p, void* const* a, void* const* b, void* out, uint32_t* tiles) {
     SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
     segment_geometry(A, a[0]);
+    if (p->bcase == BC_INFLOW) {
+        // write the next state's outflow plane exactly when the member's own
+        // step (launch_sweep) does: when it takes the one-node sweep
+        bool one_node = true;
+        if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
+            const long long ne = p->nx * p->ny * ((long long)p->n + 2) + 64;
+            if (g_pair_kernels && ne < (1LL << 31) &&
+                (pairs_aligned<S>(p, a, b) || (cm_fast(coll_mode(A)) && A.obs == nullptr)))
+                one_node = false;
+        }
+        A.outflow_next = one_node ? 1 : 0;
+    }
     SweepArgs<S, C> B = A;
     for (int d = 0; d < 18; ++d) {
         B.a[d] = (const S*)b[d];
@@ -516,7 +580,7 @@ int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n,
 #define BGK_INSTANTIATE_AB(S, C)                                                                   \
     namespace bgk {                                                                                \
     template int launch_sweep<S, C>(const bgk_sweep_params*, void* const*, void* const*, double*,  \
-                                    cudaStream_t);                                                 \
+                                    cudaStream_t, int*);                                           \
     template int launch_sweep_tma<S, C>(const bgk_sweep_params*, void* const*, void* const*,        \
                                         const void*, const int*, int*, cudaStream_t);              \
     }

@@ -182,7 +182,7 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t g
         if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
             v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force);
         if (BC == BC_INFLOW && cx == 1 && i == 1)
-            v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
+            v = Conv<S, C>::raw(P.inflow_s[d]);
         x[d] = v;
     }
     x[18] = Conv<S, C>::raw(P.a[18][c]);
@@ -225,7 +225,7 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t g
     if (BC == BC_INFLOW && i == 1) {
 #pragma unroll
         for (int d = 0; d < 5; ++d)
-            P.b[d][c] = Conv<S, C>::pack(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
+            P.b[d][c] = P.inflow_s[d];
     }
     if (BC == BC_INFLOW && i == P.l) {
         C s[19];

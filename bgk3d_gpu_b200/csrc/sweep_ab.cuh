@@ -45,6 +45,7 @@ template <class S, class C> struct SweepArgs {
     C lid_force;      // driven, storage units: added to pop 02 / subtracted from pop 11 at z = n+1
     C u_inflow;       // inflow: prescribed x velocity at x = 0
     C inflow_cte1;    // inflow equilibrium constant (0 for shifted storage)
+    S inflow_s[5];    // inflow: pops 01..05 of the x = 0 face, inflow_eq rounded to storage (host-computed)
     float scale, inv_scale;
     const int* obs;   // optional: obstacle mask, Fortran layout (1:l,1:m,1:n)
     long long obs_nx, obs_nxy;
@@ -66,13 +67,14 @@ template <class S, class C> struct SweepArgs {
     int generic;           // 1 unless the force-free shifted collision applies
     int fast;              // 1: fused-multiply-add collision (float compute only)
     int zhalo;             // bit 0 / bit 1: the face k = 1 / k = n reads the halo plane as stored
+    int outflow_next;      // inflow: nodes i = l also write the next state's outflow plane into b
 };
 
 // Equilibrium population p (0..4 -> 01..05) of the inflow face
 // (SRC/bcond.inflow.F90:165-181), in the compute type (storage units when K
 // carries the scale).
 template <class C>
-__device__ __forceinline__ C inflow_eq(int p, C u_in, C cte1, const ColConst<C>& K) {
+__host__ __device__ __forceinline__ C inflow_eq(int p, C u_in, C cte1, const ColConst<C>& K) {
     const C rf = K.rf, qf = K.qf, three = C(3), crho = C(1);
     const C xj = u_in, yj = C(0), zj = C(0);
     const C cvsq = xj * xj + yj * yj + zj * zj;
@@ -164,8 +166,13 @@ __device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j,
 // Collision of the gathered values x[] (storage units) of the node at element
 // c, the store of the new populations (b[0..17], pop 19 in place) and, with
 // P.mom, the node's moments of the stored state.
+// outflow: the node is at i = l of an inflow lattice whose launch writes
+// the next state's outflow plane (P.outflow_next): the equilibria that
+// outflow_halo_kernel would compute from this node's stored state at the
+// next step are written to b[9..13] at (l + 1, j, k) right away.
 template <class S, class C, class IDX, int CM>
-__device__ __forceinline__ void collide_store(const SweepArgs<S, C>& P, const C (&x)[19], IDX c, double (&m5)[5]) {
+__device__ __forceinline__ void collide_store(const SweepArgs<S, C>& P, const C (&x)[19], IDX c, double (&m5)[5],
+                                              bool outflow = false) {
     const float inv = P.inv_scale;
     C y[19];
     collide_cm<S, C, CM>(x, y, P.col, P.fc, inv);
@@ -175,12 +182,32 @@ __device__ __forceinline__ void collide_store(const SweepArgs<S, C>& P, const C 
 #pragma unroll
     for (int d = 0; d < 18; ++d) P.b[d][c] = sv[d];
     const_cast<S*>(P.a[18])[c] = sv[18];
+    if (outflow) {
+        C r[19];
+#pragma unroll
+        for (int d = 0; d < 19; ++d) r[d] = Conv<S, C>::raw(sv[d]);
+        C eq[5];
+        outflow_eq<C, Scaled<S>::value>(r, P.inflow_cte1, P.col, P.inv_scale, eq);
+#pragma unroll
+        for (int e = 0; e < 5; ++e) P.b[9 + e][c + 1] = Conv<S, C>::pack(eq[e]);
+    }
     if (P.mom != nullptr) {
         C s[19];
 #pragma unroll
         for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(sv[d], inv);
         diagno_node<C>(s, P.col.cte1, m5);
     }
+}
+
+// True when node (i, j, k) lies in the obstacle's box grown by one node and
+// the launch leaves that box to sweep_box_kernel: with P.obs set, an
+// obstacle-free variant (OBS = false) skips exactly the nodes whose links
+// may touch a solid node, and every other node's result is the same as with
+// the obstacle logic compiled in.
+template <class S, class C>
+__device__ __forceinline__ bool in_obstacle_box(const SweepArgs<S, C>& P, int i, int j, int k) {
+    return P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 && j <= P.jmax + 1 &&
+           k >= P.kmin - 1 && k <= P.kmax + 1;
 }
 
 // Plane mapping (P.flat): a warp owns 32 consecutive, 32-element aligned
@@ -203,6 +230,7 @@ __device__ __forceinline__ void sweep_node_flat(const SweepArgs<S, C>& P, uint32
     const int i = r - (int)jj * (int)P.nx + 1;
     const int j = (int)jj + 1;
     if (i > P.l || j > P.m) return;
+    if (!OBS && in_obstacle_box(P, i, j, k)) return;
     sweep_at<S, C, BC, IDX, CM, OBS>(P, i, j, k, m5);
 }
 
@@ -224,6 +252,7 @@ __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw
     const int sh = (int)((P.align_base + (long long)rowoff + 1) & 31);
     const int i = seg * 32 + lane + 1 - (P.nseg_aligned ? 0 : sh);
     if (i < 1 || i > P.l) return;
+    if (!OBS && in_obstacle_box(P, i, j, k)) return;
     sweep_at<S, C, BC, IDX, CM, OBS>(P, i, j, k, m5);
 }
 
@@ -270,8 +299,7 @@ __device__ __forceinline__ bool gather_at(const SweepArgs<S, C>& P, int i, int j
         C v = Conv<S, C>::raw(ldro<S>(src + (bounce ? c : off)));
         if (BC == BC_DRIVEN && (d == 1 || d == 10) && zhi)
             v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force);
-        if (BC == BC_INFLOW && cx == 1 && i == 1)
-            v = roundtrip<S, C>(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col));
+        if (BC == BC_INFLOW && cx == 1 && i == 1) v = Conv<S, C>::raw(P.inflow_s[d]);
         x[d] = v;
     }
     x[18] = Conv<S, C>::raw(P.a[18][c]);
@@ -284,7 +312,8 @@ template <class S, class C, int BC, class IDX, int CM, bool OBS>
 __device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j, int k, double (&m5)[5]) {
     C x[19];
     if (!gather_at<S, C, BC, IDX, OBS>(P, i, j, k, x)) return;
-    collide_store<S, C, IDX, CM>(P, x, (IDX)P.nx * (IDX)j + (IDX)P.nxy * (IDX)k + (IDX)i, m5);
+    collide_store<S, C, IDX, CM>(P, x, (IDX)P.nx * (IDX)j + (IDX)P.nxy * (IDX)k + (IDX)i, m5,
+                                 BC == BC_INFLOW && P.outflow_next && i == P.l);
 }
 
 // One launch = one time step.  With P.mom set (a grid of mom_grid blocks
@@ -304,6 +333,20 @@ __global__ void __launch_bounds__(256, (SweepBlocks<S, C>::value)) sweep_ab_kern
     // block (per 256 nodes it had cost as many instructions as the sums)
     for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) sweep_node<S, C, BC, IDX, CM, OBS>(P, gw, m5);
     block_reduce_store<5>(m5, P.mom);
+}
+
+// The nodes of the obstacle's box grown by one node (the box the
+// obstacle-free variant of sweep_ab_kernel skips), one per thread, i
+// fastest, with the obstacle logic compiled in.  No fused moments.
+template <class S, class C, int BC, class IDX, int CM>
+__global__ void __launch_bounds__(256, (SweepBlocks<S, C>::value)) sweep_box_kernel(const SweepArgs<S, C> P) {
+    const int i0 = P.imin - 1, j0 = P.jmin - 1, k0 = P.kmin - 1;
+    const int ni = P.imax - P.imin + 3, nj = P.jmax - P.jmin + 3, nk = P.kmax - P.kmin + 3;
+    const long long t = blockIdx.x * 256LL + threadIdx.x;
+    if (t >= (long long)ni * nj * nk) return;
+    const int i = i0 + (int)(t % ni), j = j0 + (int)((t / ni) % nj), k = k0 + (int)(t / ((long long)ni * nj));
+    double m5[5];
+    sweep_at<S, C, BC, IDX, CM, true>(P, i, j, k, m5);
 }
 
 // Two nodes per thread for the 16-bit kinds: a warp owns 64 consecutive
@@ -432,7 +475,7 @@ __device__ __forceinline__ void abp_row(const SweepArgs<S, C>& P, int j, int k, 
             const uint32_t left = __shfl_up_sync(0xffffffffu, v, 1) >> 16;
             uint32_t lo = edge_lo ? e[d] : left;
             if (BC == BC_INFLOW && at_lo)
-                lo = s_bits(Conv<S, C>::pack(inflow_eq<C>(d, P.u_inflow, P.inflow_cte1, P.col)));
+                lo = s_bits(P.inflow_s[d]);
             if (!wall[d]) v = __byte_perm(lo, v, 0x5410);
         } else if (cx == -1) {
             // node i: high half; node i + 1: lane t + 1's low half, or the edge value

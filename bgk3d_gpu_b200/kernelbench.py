@@ -79,6 +79,9 @@ def main(argv=None) -> int:
     ap.add_argument("--modes", default="strict", help="collision modes: strict, fast or both (strict,fast)")
     ap.add_argument("--tma", default="off", help="TMA-staged AB sweep: on, off or both (on,off)")
     ap.add_argument("--pair", default="on", help="two-node sweep of the 16-bit kinds: on, off or both (on,off)")
+    ap.add_argument("--split", default="off",
+                    help="obstacle cases: obstacle-free launch outside the obstacle's box + box launch "
+                         "(on), one launch with the obstacle logic (off), or both")
     args = ap.parse_args(argv)
     from ._lib import lib
     l, m, n = args.size
@@ -92,9 +95,12 @@ def main(argv=None) -> int:
                     for tma in args.tma.split(","):
                         if tma == "on" and pattern == "aa":
                             continue    # the TMA sweep serves AB lattices
-                        for pair in args.pair.split(","):
+                        for pair, split in [(p, sp) for p in args.pair.split(",") for sp in args.split.split(",")]:
                             if pair == "off" and (BYTES[kind] != 2 or tma == "on"):
                                 continue    # the two-node sweeps serve 16-bit lattices
+                            if split == "off" and case != "inflow":
+                                continue    # only the inflow case carries an obstacle
+                            prev_split = lib().bgk_set_obstacle_split(1 if split == "on" else 0)
                             prev = lib().bgk_set_tma_kernels(1 if tma == "on" else 0)
                             prev_pair = lib().bgk_set_pair_kernels(1 if pair == "on" else 0)
                             lat = make(kind, pattern, case, l, m, n, fast=(mode == "fast"))
@@ -111,9 +117,10 @@ def main(argv=None) -> int:
                             lat.close()
                             lib().bgk_set_tma_kernels(prev)
                             lib().bgk_set_pair_kernels(prev_pair)
+                            lib().bgk_set_obstacle_split(prev_split)
                             glups = l * m * n / s / 1e9
                             gbs = glups * 2 * 19 * BYTES[kind]
-                            print(json.dumps({"kind": kind, "mode": mode, "tma": tma, "path": path,
+                            print(json.dumps({"kind": kind, "mode": mode, "tma": tma, "path": path, "split": split,
                                               "status": status, "pattern": pattern, "case": case,
                                               "size": [l, m, n], "steps": args.steps, "ms_per_step": s * 1e3,
                                               "glups": glups, "hbm_gbs": gbs,

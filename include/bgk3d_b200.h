@@ -216,6 +216,15 @@ size_t bgk_abi_struct_size(int which);
    place, not only the total size.  No counterpart in the reference. */
 long long bgk_abi_field_offset(int which, int field);
 
+/* One-node AB sweep of a lattice with an obstacle, without fused moments:
+   1 runs the obstacle-free kernel variant over every node outside the
+   obstacle's box grown by one node and a second launch over that box with
+   the obstacle logic compiled in (bit-identical: only nodes in the grown box
+   can link to a solid node); 0 (default; measured 4-7 % faster on the
+   sphere case) runs one launch with the obstacle logic for every node.
+   Returns the previous setting.  No counterpart in the reference. */
+int bgk_set_obstacle_split(int enable);
+
 /* Two-node sweeps for the 16-bit kinds (FP16 / BF16 storage, FP32 compute)
    without fused moments (warps next to an obstacle advance their nodes one
    by one): every thread advances two

@@ -43,13 +43,22 @@ def test_sweep_matches_oracle(kind, case):
     assert_fluid_equal(got, want, fluid, f"kind={kind} case={case}")
 
 
+@pytest.mark.parametrize("split", [0, 1])
 @pytest.mark.parametrize("kind", [0, 1, 2])
 @pytest.mark.parametrize("case", ["driven", "periodic", "inflow", "channel"])
-def test_sweep_with_obstacle(kind, case):
-    l, m, n = 16, 14, 12
-    obs = sphere_mask(l, m, n, (7.5, 7.0, 6.2), 9.0)
-    got, want, fluid = run_pair(l, m, n, kind, case, steps=4, seed=11, obs=obs)
-    assert_fluid_equal(got, want, fluid, f"obstacle kind={kind} case={case}")
+def test_sweep_with_obstacle(kind, case, split):
+    """One launch with the obstacle logic (split 0) and the obstacle-free
+    launch outside the obstacle's grown box plus the box launch (split 1)."""
+    from bgk3d_gpu_b200 import _lib
+    L = _lib.lib()
+    prev = L.bgk_set_obstacle_split(split)
+    try:
+        l, m, n = 16, 14, 12
+        obs = sphere_mask(l, m, n, (7.5, 7.0, 6.2), 9.0)
+        got, want, fluid = run_pair(l, m, n, kind, case, steps=4, seed=11, obs=obs)
+        assert_fluid_equal(got, want, fluid, f"obstacle kind={kind} case={case} split={split}")
+    finally:
+        L.bgk_set_obstacle_split(prev)
 
 
 def test_sweep_hollow_shell_obstacle():
