@@ -119,21 +119,22 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     A.mom = mom;
     const bool fresh = halo && *halo;
     if (halo) *halo = 0;
-    bool one_node = true;   // the path below is the one-node sweep unless a pair path returns first
+    // the one-node and the adjacent-pair sweeps write the next outflow plane
+    // when asked (outflow_next); the i / i + 32 sweep (sweep_ab2_kernel) does not
+    bool writes_next = true;
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
         const long long ne = p->nx * p->ny * ((long long)p->n + 2) + 64;
-        const int cm0 = coll_mode(A);
-        if (g_pair_kernels && mom == nullptr && ne < (1LL << 31) &&
-            (pairs_aligned<S>(p, a, b) || (cm_fast(cm0) && A.obs == nullptr)))
-            one_node = false;
+        if (g_pair_kernels && mom == nullptr && ne < (1LL << 31) && !pairs_aligned<S>(p, a, b) &&
+            cm_fast(coll_mode(A)) && A.obs == nullptr)
+            writes_next = false;
     }
     if (p->bcase == BC_INFLOW) {
-        if (!fresh || !one_node) {
+        if (!fresh || !writes_next) {
             dim3 blk(128), grd((p->m + 127) / 128, p->n);
             outflow_halo_kernel<S, C><<<grd, blk, 0, st>>>(A);
             if (int e = check_launch("outflow_halo_kernel")) return e;
         }
-        if (halo && one_node) {
+        if (halo && writes_next) {
             A.outflow_next = 1;
             *halo = 1;
         }
@@ -454,15 +455,15 @@ size_t fill_batch_desc(const bgk_sweep_params* p, void* const* a, void* const* b
     segment_geometry(A, a[0]);
     if (p->bcase == BC_INFLOW) {
         // write the next state's outflow plane exactly when the member's own
-        // step (launch_sweep) does: when it takes the one-node sweep
-        bool one_node = true;
+        // step (launch_sweep) does: unless it takes the i / i + 32 sweep
+        bool writes_next = true;
         if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
             const long long ne = p->nx * p->ny * ((long long)p->n + 2) + 64;
-            if (g_pair_kernels && ne < (1LL << 31) &&
-                (pairs_aligned<S>(p, a, b) || (cm_fast(coll_mode(A)) && A.obs == nullptr)))
-                one_node = false;
+            if (g_pair_kernels && ne < (1LL << 31) && !pairs_aligned<S>(p, a, b) && cm_fast(coll_mode(A)) &&
+                A.obs == nullptr)
+                writes_next = false;
         }
-        A.outflow_next = one_node ? 1 : 0;
+        A.outflow_next = writes_next ? 1 : 0;
     }
     SweepArgs<S, C> B = A;
     for (int d = 0; d < 18; ++d) {

@@ -505,6 +505,21 @@ __device__ __forceinline__ void abp_row(const SweepArgs<S, C>& P, int j, int k, 
         bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
     else
         bgk_collide_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.col, P.inv_scale);
+    if (BC == BC_INFLOW && P.outflow_next && valid && at_hi) {
+        // node l is the high half of this lane's pair: the next state's
+        // outflow plane from the values just stored (plain loads: this
+        // thread's own stores of this launch), as outflow_halo_kernel would
+        // compute it at the next step
+        const int cl = c + 1;
+        C r[19];
+#pragma unroll
+        for (int d = 0; d < 18; ++d) r[d] = Conv<S, C>::raw(P.b[d][cl]);
+        r[18] = Conv<S, C>::raw(P.a[18][cl]);
+        C eq[5];
+        outflow_eq<C, Scaled<S>::value>(r, P.inflow_cte1, P.col, P.inv_scale, eq);
+#pragma unroll
+        for (int e = 0; e < 5; ++e) P.b[9 + e][cl + 1] = Conv<S, C>::pack(eq[e]);
+    }
 }
 
 template <class S, class C, int BC, int CM, bool OBS>
