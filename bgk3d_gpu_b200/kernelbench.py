@@ -98,8 +98,8 @@ def main(argv=None) -> int:
                         for pair, split in [(p, sp) for p in args.pair.split(",") for sp in args.split.split(",")]:
                             if pair == "off" and (BYTES[kind] != 2 or tma == "on"):
                                 continue    # the two-node sweeps serve 16-bit lattices
-                            if split == "off" and case != "inflow":
-                                continue    # only the inflow case carries an obstacle
+                            if case != "inflow" and split != args.split.split(",")[0]:
+                                continue    # only the inflow case carries an obstacle: one run
                             prev_split = lib().bgk_set_obstacle_split(1 if split == "on" else 0)
                             prev = lib().bgk_set_tma_kernels(1 if tma == "on" else 0)
                             prev_pair = lib().bgk_set_pair_kernels(1 if pair == "on" else 0)
