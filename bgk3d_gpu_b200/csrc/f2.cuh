@@ -36,6 +36,7 @@ __device__ __forceinline__ F2 operator/(F2 a, F2 b) {
 }
 __device__ __forceinline__ F2 fma_c(F2 a, F2 b, F2 c) { return F2(__ffma2_rn(a.v, b.v, c.v)); }
 __device__ __forceinline__ F2 rcp_c(F2 a) { return F2(__frcp_rn(a.v.x), __frcp_rn(a.v.y)); }
+__device__ __forceinline__ F2 inv_rn(F2 a) { return rcp_c(a); }
 
 // Storage <-> two compute values (storage units), and the 2-element vectors.
 template <class S> struct Pack2;

@@ -56,7 +56,8 @@ void by_variant(long long nelem, int cm, bool obs, A... args) {
 
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
-        sweep_ab_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
+        if (A.flat) sweep_ab_kernel<S, C, BC, IDX, CM, OBS, true><<<blocks, 256, 0, st>>>(A);
+        else sweep_ab_kernel<S, C, BC, IDX, CM, OBS, false><<<blocks, 256, 0, st>>>(A);
     }
 };
 // The obstacle's grown box (sweep_box_kernel, obstacle logic compiled in);

@@ -48,7 +48,7 @@ template <class C>
 __device__ __forceinline__ void diagno_node(const C (&x)[19], C cte1, double (&v)[5]) {
     const C rho = x[0] + x[1] + x[2] + x[3] + x[4] + x[5] + x[6] + x[7] + x[8] + x[9] + x[10] +
                   x[11] + x[12] + x[13] + x[14] + x[15] + x[16] + x[17] + x[18] + cte1;
-    const C rhoinv = rcp_c(rho);   // the correctly rounded 1 / rho
+    const C rhoinv = C(1) / rho;
     const C xj = (x[0] + x[1] + x[2] + x[3] + x[4] - x[9] - x[10] - x[11] - x[12] - x[13]) * rhoinv;
     const C yj = (x[2] + x[6] + x[7] + x[8] + x[11] - x[0] - x[9] - x[15] - x[16] - x[17]) * rhoinv;
     const C zj = (x[3] + x[5] + x[6] + x[12] + x[17] - x[1] - x[8] - x[10] - x[14] - x[15]) * rhoinv;

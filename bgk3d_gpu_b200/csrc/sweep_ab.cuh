@@ -215,43 +215,46 @@ __device__ __forceinline__ bool in_obstacle_box(const SweepArgs<S, C>& P, int i,
 // one z plane, rows back to back.  Lanes that land on a halo column (i = 0 or
 // i > l) idle: 2 of every nx lanes on the reference's nx = l + 2 layout,
 // where whole rows would cost one extra warp per row (9 warps for 256 nodes).
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
-__device__ __forceinline__ void sweep_node_flat(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
+// Row mapping (otherwise): a warp owns 32 elements of one (j, k) row.
+// Returns false for a lane without a node.  FLAT selects the plane mapping
+// at compile time (a run-time choice between the two made the compiler lay
+// out some variants of the sweep 12 % slower).
+template <class S, class C, class IDX, bool FLAT>
+__device__ __forceinline__ bool warp_node(const SweepArgs<S, C>& P, uint32_t gw, int& i, int& j, int& k) {
     const int lane = threadIdx.x & 31;
-    const uint32_t kk = P.div_fw.div(gw);
-    if (kk >= (uint32_t)P.n) return;
-    const int s = (int)(gw - kk * P.fwpp);
-    const int k = (int)kk + 1;
-    const IDX first = (IDX)P.nx + (IDX)P.nxy * (IDX)k + 1;   // element of node (1, 1, k)
-    const int sh = (int)((P.align_base + (long long)first) & 31);
-    const int r = s * 32 + lane - sh;                      // element offset from node (1, 1, k)
-    if (r < 0) return;
-    const uint32_t jj = P.div_nx.div((uint32_t)r);
-    const int i = r - (int)jj * (int)P.nx + 1;
-    const int j = (int)jj + 1;
-    if (i > P.l || j > P.m) return;
-    if (!OBS && in_obstacle_box(P, i, j, k)) return;
-    sweep_at<S, C, BC, IDX, CM, OBS>(P, i, j, k, m5);
-}
-
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
-__device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
-    if (P.flat) {
-        sweep_node_flat<S, C, BC, IDX, CM, OBS>(P, gw, m5);
-        return;
+    const IDX nx = (IDX)P.nx, nxy = (IDX)P.nxy;
+    if constexpr (FLAT) {
+        const uint32_t kk = P.div_fw.div(gw);
+        if (kk >= (uint32_t)P.n) return false;
+        const int s = (int)(gw - kk * P.fwpp);
+        k = (int)kk + 1;
+        const IDX first = nx + nxy * (IDX)k + 1;            // element of node (1, 1, k)
+        const int sh = (int)((P.align_base + (long long)first) & 31);
+        const int r = s * 32 + lane - sh;                    // element offset from node (1, 1, k)
+        if (r < 0) return false;
+        const uint32_t jj = P.div_nx.div((uint32_t)r);
+        i = r - (int)jj * (int)P.nx + 1;
+        j = (int)jj + 1;
+        return i <= P.l && j <= P.m;
     }
-    const int lane = threadIdx.x & 31;
     const uint32_t row = P.div_seg.div(gw);
-    if (row >= P.nrows) return;
+    if (row >= P.nrows) return false;
     const int seg = (int)(gw - row * (uint32_t)P.nseg);
     const uint32_t kk = P.div_m.div(row);
-    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
-    const int k = (int)kk + 1;
-    const IDX nx = (IDX)P.nx, nxy = (IDX)P.nxy;
+    j = (int)(row - kk * (uint32_t)P.m) + 1;
+    k = (int)kk + 1;
     const IDX rowoff = nx * (IDX)j + nxy * (IDX)k;
     const int sh = (int)((P.align_base + (long long)rowoff + 1) & 31);
-    const int i = seg * 32 + lane + 1 - (P.nseg_aligned ? 0 : sh);
-    if (i < 1 || i > P.l) return;
+    i = seg * 32 + lane + 1 - (P.nseg_aligned ? 0 : sh);
+    return i >= 1 && i <= P.l;
+}
+
+// The node of this lane under the warp-segment mapping (FLAT: the plane
+// mapping, which the launch selects when P.flat is set), and its time step.
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool FLAT = false>
+__device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
+    int i, j, k;
+    if (!warp_node<S, C, IDX, FLAT>(P, gw, i, j, k)) return;
     if (!OBS && in_obstacle_box(P, i, j, k)) return;
     sweep_at<S, C, BC, IDX, CM, OBS>(P, i, j, k, m5);
 }
@@ -320,18 +323,18 @@ __device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j,
 // striding over the warps), every block also writes the
 // FP64 sums of SRC/diagno.F90's per-node moments of the state it produced
 // (fluid nodes) to P.mom[blockIdx.x * 5 ..].
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool FLAT>
 __global__ void __launch_bounds__(256, (SweepBlocks<S, C>::value)) sweep_ab_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const uint32_t w0 = blockIdx.x * 8u + (threadIdx.x >> 5);
     if (P.mom == nullptr) {
-        sweep_node<S, C, BC, IDX, CM, OBS>(P, w0, m5);
+        sweep_node<S, C, BC, IDX, CM, OBS, FLAT>(P, w0, m5);
         return;
     }
     // with moments: a fixed grid strides over the step's warps, so each
     // thread accumulates many nodes and the block reduction runs once per
     // block (per 256 nodes it had cost as many instructions as the sums)
-    for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) sweep_node<S, C, BC, IDX, CM, OBS>(P, gw, m5);
+    for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) sweep_node<S, C, BC, IDX, CM, OBS, FLAT>(P, gw, m5);
     block_reduce_store<5>(m5, P.mom);
 }
 
