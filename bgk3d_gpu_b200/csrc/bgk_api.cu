@@ -53,20 +53,20 @@ long long sweep_blocks(const bgk_sweep_params* p, const void* a0, bool one_node_
     const long long align = a0 ? (long long)(((uintptr_t)a0 / es) & 31) : 0;
     const long long warps = a0 ? seg_plan(p->l, p->m, p->n, p->nx, align, one_node_ab).warps
                                : (long long)((p->l + 62) / 32) * p->m * p->n;
-    return mom_grid((warps + 7) / 8);
+    return mom_plan(warps).blocks;
 }
 
-long long mom_grid(long long blocks) {
-    static int nsm[64] = {0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int& n = nsm[dev >= 0 && dev < 64 ? dev : 0];
-    if (n == 0) {
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 1;
-    }
-    const long long g = 20LL * n;
-    return blocks < g ? blocks : g;
+MomPlan mom_plan(long long warps) {
+    // Runs of 64 segments (eight rounds of a block's 8 warps, 2048 nodes)
+    // keep the partials few enough for one finalizing block; blocks that
+    // stride over the lattice or live longer run slower (measured on the
+    // 256^3 FP32 step, B200: grids of 4 / 20 / 80 blocks per SM striding,
+    // 596 / 498 / 473 us; runs of 64 segments 471 us; the step without
+    // moments 441 us; shorter runs in the last wave changed nothing).
+    MomPlan m;
+    m.span = 64;
+    m.blocks = (warps + m.span - 1) / m.span;
+    return m;
 }
 
 int finalize_moments(const double* partials, long long nparts, double* out, cudaStream_t st) {

@@ -64,7 +64,13 @@ int sweep_launch_mom(const struct bgk_sweep_params* p, void* const* a, void* con
 // blocks per SM of the current device, fewer for small lattices) strides over
 // the step's warps.  The partial sums, and so the last bits of the moments,
 // depend on the device's SM count, never on timing.
-long long mom_grid(long long blocks);
+// Grid of a time-step launch that also sums moments, over `warps` warp
+// segments: block b advances the run of span segments from b * span
+// (block_segments, reduce.cuh); span is a multiple of 8.
+struct MomPlan {
+    long long blocks, span;
+};
+MomPlan mom_plan(long long warps);
 // Number of blocks (= partial-moment slots) of the sweep launch with moments
 // for p with population 01 at a0 (nullptr: the upper bound for any alignment);
 // one_node_ab: the launch is the one-node AB sweep (plane mapping allowed),

@@ -56,8 +56,13 @@ void by_variant(long long nelem, int cm, bool obs, A... args) {
 
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AbLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
-        if (A.flat) sweep_ab_kernel<S, C, BC, IDX, CM, OBS, true><<<blocks, 256, 0, st>>>(A);
-        else sweep_ab_kernel<S, C, BC, IDX, CM, OBS, false><<<blocks, 256, 0, st>>>(A);
+        if (A.mom) {
+            if (A.flat) sweep_ab_kernel<S, C, BC, IDX, CM, OBS, true, true><<<blocks, 256, 0, st>>>(A);
+            else sweep_ab_kernel<S, C, BC, IDX, CM, OBS, false, true><<<blocks, 256, 0, st>>>(A);
+        } else {
+            if (A.flat) sweep_ab_kernel<S, C, BC, IDX, CM, OBS, true, false><<<blocks, 256, 0, st>>>(A);
+            else sweep_ab_kernel<S, C, BC, IDX, CM, OBS, false, false><<<blocks, 256, 0, st>>>(A);
+        }
     }
 };
 // The obstacle's grown box (sweep_box_kernel, obstacle logic compiled in);
@@ -93,12 +98,14 @@ bool pairs_aligned(const bgk_sweep_params* p, void* const* a, void* const* b) {
 }
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AaEvenLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
-        aa_even_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
+        if (A.mom) aa_even_kernel<S, C, BC, IDX, CM, OBS, true><<<blocks, 256, 0, st>>>(A);
+        else aa_even_kernel<S, C, BC, IDX, CM, OBS, false><<<blocks, 256, 0, st>>>(A);
     }
 };
 template <class S, class C, int BC, class IDX, int CM, bool OBS> struct AaOddLaunch {
     static void go(const SweepArgs<S, C>& A, unsigned blocks, cudaStream_t st) {
-        aa_odd_kernel<S, C, BC, IDX, CM, OBS><<<blocks, 256, 0, st>>>(A);
+        if (A.mom) aa_odd_kernel<S, C, BC, IDX, CM, OBS, true><<<blocks, 256, 0, st>>>(A);
+        else aa_odd_kernel<S, C, BC, IDX, CM, OBS, false><<<blocks, 256, 0, st>>>(A);
     }
 };
 
@@ -146,7 +153,9 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
     const int cm = coll_mode(A);
     const bool obs = A.obs != nullptr;
-    const unsigned nb = (unsigned)(mom ? mom_grid(blocks) : blocks);
+    const MomPlan mp = mom_plan(warps);
+    A.mom_span = (uint32_t)mp.span;
+    const unsigned nb = (unsigned)(mom ? mp.blocks : blocks);
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
         if (g_pair_kernels && mom == nullptr && nelem < (1LL << 31) && pairs_aligned<S>(p, a, b)) {
             // adjacent node pairs: 64-node segments from i = 1
@@ -399,7 +408,9 @@ int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* m
     A.mom = mom;
     const long long warps = (long long)A.nseg * p->m * p->n;
     if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
-    const unsigned blocks = (unsigned)(mom ? mom_grid((warps + 7) / 8) : (warps + 7) / 8);
+    const MomPlan mp = mom_plan(warps);
+    A.mom_span = (uint32_t)mp.span;
+    const unsigned blocks = (unsigned)(mom ? mp.blocks : (warps + 7) / 8);
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
         const int cm = coll_mode(A);

@@ -42,6 +42,24 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NQ], double* part
     }
 }
 
+// The warp segments [beg, end) that block blockIdx.x of a time-step launch
+// that also sums moments advances (the grid of mom_plan): the contiguous run
+// of span segments from blockIdx.x * span.  The block's warps interleave
+// (warp w takes beg + w, beg + w + 8, ...), so neighbouring segments, which
+// share the DRAM sectors of their c_x = +-1 links, run at about the same
+// time.  (A grid stride over the whole lattice let the warps drift apart:
+// measured 13 % slower than the step without moments at 256^3 FP32.)
+struct SegRun {
+    uint32_t beg, end;
+};
+__device__ __forceinline__ SegRun block_segments(uint32_t nwarps, uint32_t span) {
+    const unsigned long long beg = (unsigned long long)span * blockIdx.x, end = beg + span;
+    SegRun r;
+    r.beg = (uint32_t)(beg < nwarps ? beg : nwarps);
+    r.end = (uint32_t)(end < nwarps ? end : nwarps);
+    return r;
+}
+
 // Per-node diagnostics of SRC/diagno.F90:112-127 (rho, u in the compute
 // type) accumulated into FP64: v += {rho, u_x, u_y, u_z, 0.5|u|^2}.
 template <class C>
@@ -129,16 +147,16 @@ __global__ void __launch_bounds__(256) draglift_partial_kernel(const FieldArgs<S
 
 // Second pass: one block sums nparts partials of NQ values in a fixed order.
 // Thread t adds partials t, t + T, t + 2T, ... in that order (T = 512, so
-// that the four records in flight fit in registers), four loads in flight at
-// a time (a partial array of the fused-moments sweep at
-// 256^3 holds ~74 K records: one strided load at a time per thread made this
-// pass ~0.2 ms, as long as the sweep); then the threads' sums are combined
-// by a fixed shuffle tree and the warps' in warp order.
+// that the eight records in flight fit in registers), eight records in
+// flight at a time (the fused-moments sweep at 256^3 leaves ~8 K records:
+// this pass is a few microseconds of latency, two rounds of loads); then the
+// threads' sums are combined by a fixed shuffle tree and the warps' in warp
+// order.
 constexpr int kFinalizeThreads = 512;
 template <int NQ>
 __global__ void __launch_bounds__(kFinalizeThreads) finalize_partials_kernel(const double* partial, long long nparts,
                                                                              double* out) {
-    constexpr int T = kFinalizeThreads, U = 4;
+    constexpr int T = kFinalizeThreads, U = 8;
     __shared__ double sm[T / 32][NQ];
     double v[NQ];
 #pragma unroll

@@ -52,7 +52,7 @@ __device__ __forceinline__ bool aa_node(const SweepArgs<S, C>& P, uint32_t gw, i
 
 // Even (local) step.  P.a and P.b both name the slot arrays.  Arithmetic in
 // storage units, as in sweep_node.
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
 __device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
     int i, j, k;
     IDX c;
@@ -82,7 +82,7 @@ __device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, uint32_t 
 #pragma unroll
         for (int e = 0; e < 5; ++e) P.b[opp_of(9 + e)][c + 1] = Conv<S, C>::pack(eq[e]);
     }
-    if (P.mom != nullptr) {
+    if constexpr (MOM) {
         C s[19];
 #pragma unroll
         for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(st[d], inv);
@@ -90,16 +90,17 @@ __device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, uint32_t 
     }
 }
 
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const uint32_t w0 = blockIdx.x * 8u + (threadIdx.x >> 5);
-    if (P.mom == nullptr) {
-        aa_even_node<S, C, BC, IDX, CM, OBS>(P, w0, m5);
-        return;
+    if constexpr (!MOM) {
+        aa_even_node<S, C, BC, IDX, CM, OBS, false>(P, blockIdx.x * 8u + (threadIdx.x >> 5), m5);
+    } else {
+        const SegRun r = block_segments(P.nwarps, P.mom_span);
+        for (uint32_t gw = r.beg + (threadIdx.x >> 5); gw < r.end; gw += 8u)
+            aa_even_node<S, C, BC, IDX, CM, OBS, true>(P, gw, m5);
+        block_reduce_store<5>(m5, P.mom);
     }
-    for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) aa_even_node<S, C, BC, IDX, CM, OBS>(P, gw, m5);
-    block_reduce_store<5>(m5, P.mom);
 }
 
 // Even step of the 16-bit kinds on aligned pairs
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel
 }
 
 // Odd (pull + push) step.
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
 __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
     typedef Faces<BC> F;
     int i, j, k;
@@ -216,7 +217,7 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t g
         }
     }
     P.b[18][c] = sv[18];
-    if (P.mom != nullptr) {
+    if constexpr (MOM) {
         C s[19];
 #pragma unroll
         for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(sv[d], inv);
@@ -244,16 +245,17 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t g
     }
 }
 
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const uint32_t w0 = blockIdx.x * 8u + (threadIdx.x >> 5);
-    if (P.mom == nullptr) {
-        aa_odd_node<S, C, BC, IDX, CM, OBS>(P, w0, m5);
-        return;
+    if constexpr (!MOM) {
+        aa_odd_node<S, C, BC, IDX, CM, OBS, false>(P, blockIdx.x * 8u + (threadIdx.x >> 5), m5);
+    } else {
+        const SegRun r = block_segments(P.nwarps, P.mom_span);
+        for (uint32_t gw = r.beg + (threadIdx.x >> 5); gw < r.end; gw += 8u)
+            aa_odd_node<S, C, BC, IDX, CM, OBS, true>(P, gw, m5);
+        block_reduce_store<5>(m5, P.mom);
     }
-    for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) aa_odd_node<S, C, BC, IDX, CM, OBS>(P, gw, m5);
-    block_reduce_store<5>(m5, P.mom);
 }
 
 // Odd step of the 16-bit kinds on aligned pairs (the layout of

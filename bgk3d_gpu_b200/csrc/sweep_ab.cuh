@@ -63,6 +63,7 @@ template <class S, class C> struct SweepArgs {
     uint32_t fwpp;         // warps per z plane
     FastDiv div_fw, div_nx;
     double* mom;           // optional: per-block FP64 partial moments of the new state
+    uint32_t mom_span;     // with mom: segments per block (mom_plan), a multiple of 8
     int bcase;             // BC_* (used by the batched kernel, which dispatches per tile)
     int generic;           // 1 unless the force-free shifted collision applies
     int fast;              // 1: fused-multiply-add collision (float compute only)
@@ -160,17 +161,18 @@ __device__ __forceinline__ uint32_t obstacle_links(const SweepArgs<S, C>& P, int
 // gw: this warp's global segment index within the lattice.
 // CM: collision mode; OBS: the lattice may have an obstacle (P.obs is then
 // tested at run time; OBS = false compiles the obstacle logic out).
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM = false>
 __device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j, int k, double (&m5)[5]);
 
 // Collision of the gathered values x[] (storage units) of the node at element
 // c, the store of the new populations (b[0..17], pop 19 in place) and, with
-// P.mom, the node's moments of the stored state.
+// MOM (the launch sums moments into P.mom), the node's moments of the stored
+// state.
 // outflow: the node is at i = l of an inflow lattice whose launch writes
 // the next state's outflow plane (P.outflow_next): the equilibria that
 // outflow_halo_kernel would compute from this node's stored state at the
 // next step are written to b[9..13] at (l + 1, j, k) right away.
-template <class S, class C, class IDX, int CM>
+template <class S, class C, class IDX, int CM, bool MOM>
 __device__ __forceinline__ void collide_store(const SweepArgs<S, C>& P, const C (&x)[19], IDX c, double (&m5)[5],
                                               bool outflow = false) {
     const float inv = P.inv_scale;
@@ -191,7 +193,7 @@ __device__ __forceinline__ void collide_store(const SweepArgs<S, C>& P, const C 
 #pragma unroll
         for (int e = 0; e < 5; ++e) P.b[9 + e][c + 1] = Conv<S, C>::pack(eq[e]);
     }
-    if (P.mom != nullptr) {
+    if constexpr (MOM) {
         C s[19];
 #pragma unroll
         for (int d = 0; d < 19; ++d) s[d] = Conv<S, C>::ld(sv[d], inv);
@@ -250,13 +252,14 @@ __device__ __forceinline__ bool warp_node(const SweepArgs<S, C>& P, uint32_t gw,
 }
 
 // The node of this lane under the warp-segment mapping (FLAT: the plane
-// mapping, which the launch selects when P.flat is set), and its time step.
-template <class S, class C, int BC, class IDX, int CM, bool OBS, bool FLAT = false>
+// mapping, which the launch selects when P.flat is set), and its time step
+// (MOM: with the node's moments added to m5).
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool FLAT = false, bool MOM = false>
 __device__ __forceinline__ void sweep_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
     int i, j, k;
     if (!warp_node<S, C, IDX, FLAT>(P, gw, i, j, k)) return;
     if (!OBS && in_obstacle_box(P, i, j, k)) return;
-    sweep_at<S, C, BC, IDX, CM, OBS>(P, i, j, k, m5);
+    sweep_at<S, C, BC, IDX, CM, OBS, MOM>(P, i, j, k, m5);
 }
 
 // The 19 pulled values (storage units) of interior node (i, j, k), 1 <= i <= l
@@ -310,32 +313,34 @@ __device__ __forceinline__ bool gather_at(const SweepArgs<S, C>& P, int i, int j
 }
 
 // The time step of interior node (i, j, k): gather, collision, store and
-// (with P.mom) the node's moments.
-template <class S, class C, int BC, class IDX, int CM, bool OBS>
+// (MOM) the node's moments.
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
 __device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j, int k, double (&m5)[5]) {
     C x[19];
     if (!gather_at<S, C, BC, IDX, OBS>(P, i, j, k, x)) return;
-    collide_store<S, C, IDX, CM>(P, x, (IDX)P.nx * (IDX)j + (IDX)P.nxy * (IDX)k + (IDX)i, m5,
+    collide_store<S, C, IDX, CM, MOM>(P, x, (IDX)P.nx * (IDX)j + (IDX)P.nxy * (IDX)k + (IDX)i, m5,
                                  BC == BC_INFLOW && P.outflow_next && i == P.l);
 }
 
-// One launch = one time step.  With P.mom set (a grid of mom_grid blocks
-// striding over the warps), every block also writes the
-// FP64 sums of SRC/diagno.F90's per-node moments of the state it produced
-// (fluid nodes) to P.mom[blockIdx.x * 5 ..].
-template <class S, class C, int BC, class IDX, int CM, bool OBS, bool FLAT>
+// One launch = one time step.  MOM (the launch has P.mom set and the grid of
+// mom_plan, each block advancing one contiguous run of segments): every
+// block also writes the FP64 sums of SRC/diagno.F90's per-node moments of
+// the state it produced (fluid nodes) to P.mom[blockIdx.x * 5 ..].  The two
+// forms are separate kernels: as one kernel with a run-time branch, changes
+// to either path moved the other's speed by up to 9 % (code layout).
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool FLAT, bool MOM>
 __global__ void __launch_bounds__(256, (SweepBlocks<S, C>::value)) sweep_ab_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const uint32_t w0 = blockIdx.x * 8u + (threadIdx.x >> 5);
-    if (P.mom == nullptr) {
-        sweep_node<S, C, BC, IDX, CM, OBS, FLAT>(P, w0, m5);
-        return;
+    if constexpr (!MOM) {
+        sweep_node<S, C, BC, IDX, CM, OBS, FLAT, false>(P, blockIdx.x * 8u + (threadIdx.x >> 5), m5);
+    } else {
+        // several nodes per thread and one block reduction per run (once per
+        // 256 nodes it had cost as many instructions as the sums)
+        const SegRun r = block_segments(P.nwarps, P.mom_span);
+        for (uint32_t gw = r.beg + (threadIdx.x >> 5); gw < r.end; gw += 8u)
+            sweep_node<S, C, BC, IDX, CM, OBS, FLAT, true>(P, gw, m5);
+        block_reduce_store<5>(m5, P.mom);
     }
-    // with moments: a fixed grid strides over the step's warps, so each
-    // thread accumulates many nodes and the block reduction runs once per
-    // block (per 256 nodes it had cost as many instructions as the sums)
-    for (uint32_t gw = w0; gw < P.nwarps; gw += gridDim.x * 8u) sweep_node<S, C, BC, IDX, CM, OBS, FLAT>(P, gw, m5);
-    block_reduce_store<5>(m5, P.mom);
 }
 
 // The nodes of the obstacle's box grown by one node (the box the
