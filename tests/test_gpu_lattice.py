@@ -49,6 +49,30 @@ def test_lattice_matches_oracle(pattern, kind, case):
     assert_fluid_equal(got, want, fluid, f"{pattern} kind={kind} case={case}")
 
 
+@pytest.mark.parametrize("kind,pair", [(0, True), (1, True), (2, True), (2, False), (3, False)])
+@pytest.mark.parametrize("case", CASES)
+def test_aa_interior_warps_match_oracle(kind, pair, case):
+    """70-node rows: every row holds a warp of nodes (33..64) that lies wholly
+    inside the x faces next to warps that touch them, which the 13-node rows
+    above never do (16-bit kinds: also the one-node AA steps, with the pair
+    steps switched off)."""
+    from bgk3d_gpu_b200 import _lib
+    prev = _lib.lib().bgk_set_pair_kernels(1 if pair else 0)
+    try:
+        got, want, fluid = run_pair(70, 6, 5, kind, case, "aa", steps=4, seed=23 + kind)
+    finally:
+        _lib.lib().bgk_set_pair_kernels(prev)
+    assert_fluid_equal(got, want, fluid, f"aa interior kind={kind} case={case}")
+
+
+@pytest.mark.parametrize("case", ["driven", "periodic", "inflow", "channel"])
+def test_aa_interior_warps_with_obstacle(case):
+    l, m, n = 70, 9, 8
+    obs = sphere_mask(l, m, n, (40.0, 5.0, 4.5), 4.0)
+    got, want, fluid = run_pair(l, m, n, 1, case, "aa", steps=6, seed=31, obs=obs)
+    assert_fluid_equal(got, want, fluid, f"aa interior obstacle case={case}")
+
+
 @pytest.mark.parametrize("pattern", ["ab", "aa"])
 @pytest.mark.parametrize("case", ["driven", "periodic", "inflow", "channel"])
 def test_lattice_obstacle(pattern, case):
