@@ -167,6 +167,10 @@ def load_dropin(double: bool) -> ctypes.CDLL:
     D.bgk_dropin_track_moments.restype = None
     D.bgk_dropin_moments.argtypes = [c_void_p, c_void_p]
     D.bgk_dropin_moments.restype = c_int
+    D.bgk_dropin_moments_ptr.argtypes = []
+    D.bgk_dropin_moments_ptr.restype = c_void_p
+    D.bgk_dropin_moments_to.argtypes = [c_void_p]
+    D.bgk_dropin_moments_to.restype = None
     for f in ("bcond_periodic_gpu", "bcond_channel_gpu", "bcond_driven_gpu", "bcond_inflow_gpu",
               "bcond_obs_gpu", "gpu_device_sync", "bgk_dropin_reset", "bgk_dropin_track_moments"):
         getattr(D, f).restype = None

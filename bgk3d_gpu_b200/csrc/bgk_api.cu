@@ -124,8 +124,8 @@ int bgk::sweep_launch(const bgk_sweep_params* p, void* const* a, void* const* b,
 }
 
 int bgk::sweep_launch_mom(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom,
-                          cudaStream_t st, int* halo) {
-    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, mom, st, halo)));
+                          cudaStream_t st, int* halo, double* mom_out, unsigned* mom_ticket) {
+    KIND_DISPATCH(p->kind, (launch_sweep<S, C>(p, a, b, mom, st, halo, mom_out, mom_ticket)));
 }
 
 int bgk::dissipation_launch(const bgk_sweep_params* p, void* const* a, double nu, double* out, double* ws,
@@ -183,7 +183,7 @@ int bgk_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, void* s
 
 size_t bgk_sweep_moments_workspace_bytes(const bgk_sweep_params* p) {
     if (!p) return 0;
-    return (size_t)bgk::sweep_blocks(p, nullptr) * 5 * sizeof(double);
+    return bgk::fused_workspace_bytes(bgk::sweep_blocks(p, nullptr), 5);
 }
 
 int bgk_sweep_moments(const bgk_sweep_params* p, void* const* a, void* const* b, double* out_dev, void* workspace,
@@ -192,12 +192,15 @@ int bgk_sweep_moments(const bgk_sweep_params* p, void* const* a, void* const* b,
     if (!a || !b || !out_dev || !workspace) return set_error(BGK_ERR_ARG, "null pointer");
     for (int d = 0; d < 19; ++d)
         if (!a[d] || (d < 18 && !b[d])) return set_error(BGK_ERR_ARG, "null population %d", d + 1);
-    const long long nb = bgk::sweep_blocks(p, a[0]);
-    if (workspace_bytes < (size_t)nb * 5 * sizeof(double))
-        return set_error(BGK_ERR_ARG, "workspace too small: %zu < %zu", workspace_bytes, (size_t)nb * 40);
+    const long long nb_max = bgk::sweep_blocks(p, nullptr);
+    const size_t need = bgk::fused_workspace_bytes(nb_max, 5);
+    if (workspace_bytes < need) return set_error(BGK_ERR_ARG, "workspace too small: %zu < %zu", workspace_bytes, need);
     cudaStream_t st = (cudaStream_t)stream;
-    if (int rc = bgk::sweep_launch_mom(p, a, b, (double*)workspace, st)) return rc;
-    return bgk::finalize_moments((const double*)workspace, nb, out_dev, st);
+    const bgk::FusedWs fw = bgk::fused_ws(workspace, nb_max);
+    // the caller's workspace holds anything: clear the counters
+    cudaError_t e = cudaMemsetAsync(fw.tickets, 0, bgk::fused_ticket_bytes(nb_max), st);
+    if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
+    return bgk::sweep_launch_mom(p, a, b, fw.records, st, nullptr, out_dev, fw.tickets);
 }
 
 size_t bgk_reduce_workspace_bytes(int l, int m, int n) {
@@ -249,20 +252,21 @@ int bgk_device_sync(void) {
     return BGK_OK;
 }
 
-int bgk_dropin_sweep_tracked(const bgk_sweep_params* p, void* const* a, void* const* b, double* partials,
-                             size_t bytes, long long* nparts) {
-    if (int e = validate(p)) return e;
-    const long long nb = bgk::sweep_blocks(p, a[0]);
-    if (!partials || bytes < (size_t)nb * 5 * sizeof(double)) {
-        *nparts = 0;
-        return bgk::sweep_launch(p, a, b, nullptr);
-    }
-    *nparts = nb;
-    return bgk::sweep_launch_mom(p, a, b, partials, nullptr);
+size_t bgk_dropin_tracked_workspace_bytes(const bgk_sweep_params* p) {
+    if (!p) return 0;
+    return bgk::fused_workspace_bytes(bgk::sweep_blocks(p, nullptr), 5);
 }
 
-int bgk_dropin_finalize(const double* partials, long long nparts, double* out_dev, void* stream) {
-    return bgk::finalize_moments(partials, nparts, out_dev, (cudaStream_t)stream);
+int bgk_dropin_sweep_tracked(const bgk_sweep_params* p, void* const* a, void* const* b, void* workspace,
+                             size_t bytes, double* out_dev) {
+    if (int e = validate(p)) return e;
+    if (!a || !b || !workspace || !out_dev) return set_error(BGK_ERR_ARG, "null pointer");
+    const long long nb_max = bgk::sweep_blocks(p, nullptr);
+    if (bytes < bgk::fused_workspace_bytes(nb_max, 5))
+        return set_error(BGK_ERR_ARG, "workspace too small: %zu < %zu", bytes,
+                         bgk::fused_workspace_bytes(nb_max, 5));
+    const bgk::FusedWs fw = bgk::fused_ws(workspace, nb_max);
+    return bgk::sweep_launch_mom(p, a, b, fw.records, nullptr, nullptr, out_dev, fw.tickets);
 }
 
 const char* bgk_last_error(void) { return g_last_error.c_str(); }

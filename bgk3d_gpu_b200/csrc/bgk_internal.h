@@ -57,13 +57,13 @@ int moments_launch(const struct bgk_sweep_params* p, void* const* a, double* out
 int sweep_launch(const struct bgk_sweep_params* p, void* const* a, void* const* b, cudaStream_t st);
 // Same, with the per-block FP64 moments of the new state written to mom;
 // halo (inflow, nullable): in, a's outflow plane is fresh (no pre-pass); out,
-// the launch wrote the next state's outflow plane into b.
+// the launch wrote the next state's outflow plane into b.  With mom (the
+// records of fused_ws, reduce.cuh), mom_out and mom_ticket (its counters,
+// zero before the launch and left zero) are required: the launch sums the
+// moments into mom_out[0..4] itself (finalize_by_tickets).
 int sweep_launch_mom(const struct bgk_sweep_params* p, void* const* a, void* const* b, double* mom,
-                     cudaStream_t st, int* halo = nullptr);
-// Blocks of a sweep launch that also produces moments: a fixed grid (20
-// blocks per SM of the current device, fewer for small lattices) strides over
-// the step's warps.  The partial sums, and so the last bits of the moments,
-// depend on the device's SM count, never on timing.
+                     cudaStream_t st, int* halo = nullptr, double* mom_out = nullptr,
+                     unsigned* mom_ticket = nullptr);
 // Grid of a time-step launch that also sums moments, over `warps` warp
 // segments: block b advances the run of span segments from b * span
 // (block_segments, reduce.cuh); span is a multiple of 8.
@@ -71,7 +71,7 @@ struct MomPlan {
     long long blocks, span;
 };
 MomPlan mom_plan(long long warps);
-// Number of blocks (= partial-moment slots) of the sweep launch with moments
+// Number of blocks (= moment records) of the sweep launch with moments
 // for p with population 01 at a0 (nullptr: the upper bound for any alignment);
 // one_node_ab: the launch is the one-node AB sweep (plane mapping allowed),
 // false for the AA steps.

@@ -23,12 +23,16 @@ struct Pending {
 };
 thread_local Pending g_pending;
 
-// Optional FP64 moments of the state each col_mc_gpu writes (same pass).
+// Optional FP64 moments of the state each col_mc_gpu writes (same launch).
 struct Tracked {
     bool on = false;
-    double* partials = nullptr;
-    size_t bytes = 0;
-    long long nparts = 0;
+    void* ws = nullptr;        // workspace of bgk_dropin_sweep_tracked, then the five sums
+    size_t bytes = 0;          // workspace bytes (a multiple of 8)
+    double* own = nullptr;     // the library's five-double target (device memory, after ws)
+    double* next = nullptr;    // target of the next tracked step (bgk_dropin_moments_to), else own
+    double* sums = nullptr;    // where the last tracked step wrote its moments
+    bool valid = false;        // sums hold a tracked step's moments
+    long long shape[6] = {};   // lattice shape the workspace was zeroed for
 };
 thread_local Tracked g_tracked;
 
@@ -136,17 +140,36 @@ void col_mc_gpu(const real_t* a01, const real_t* a02, const real_t* a03, const r
     g.has_obs = false;
     int rc;
     Tracked& t = g_tracked;
+    t.valid = false;
     if (t.on) {
-        const size_t need = bgk_sweep_moments_workspace_bytes(&p);
+        const size_t need = (bgk_dropin_tracked_workspace_bytes(&p) + 7) / 8 * 8;
+        const long long shape[6] = {p.kind, l, m, n, nx, ny};
+        bool zero = std::memcmp(shape, t.shape, sizeof shape) != 0;
         if (t.bytes < need) {
-            if (t.partials) cudaFree(t.partials);
-            t.partials = nullptr; t.bytes = 0;
-            if (cudaMalloc(&t.partials, need) == cudaSuccess) t.bytes = need;
+            if (t.ws) cudaFree(t.ws);
+            t.ws = nullptr; t.bytes = 0; t.own = nullptr;
+            if (cudaMalloc(&t.ws, need + 5 * sizeof(double)) == cudaSuccess) {
+                t.bytes = need;
+                t.own = reinterpret_cast<double*>(static_cast<char*>(t.ws) + need);
+            }
+            zero = true;
         }
-        rc = bgk_dropin_sweep_tracked(&p, a, b, t.partials, t.bytes, &t.nparts);
+        // the workspace's counters start at zero for each lattice shape
+        if (t.ws && zero && cudaMemsetAsync(t.ws, 0, t.bytes, nullptr) == cudaSuccess)
+            std::memcpy(t.shape, shape, sizeof shape);
+        else if (zero)
+            t.bytes = 0;
+        if (t.ws && t.bytes) {
+            t.sums = t.next ? t.next : t.own;
+            rc = bgk_dropin_sweep_tracked(&p, a, b, t.ws, t.bytes, t.sums);
+            t.valid = rc == BGK_OK;
+        } else {
+            rc = bgk_sweep(&p, a, b, nullptr);
+        }
     } else {
         rc = bgk_sweep(&p, a, b, nullptr);
     }
+    t.next = nullptr;
     if (rc != BGK_OK) {
         fprintf(stderr, "ERROR: col_mc_gpu: %s\n", bgk_last_error());
         fflush(stderr);
@@ -164,15 +187,23 @@ void gpu_device_sync(void) {
 
 void bgk_dropin_reset(void) {
     g_pending = Pending();
-    if (g_tracked.partials) cudaFree(g_tracked.partials);
+    if (g_tracked.ws) cudaFree(g_tracked.ws);
     g_tracked = Tracked();
 }
 
 void bgk_dropin_track_moments(int on) { g_tracked.on = (on != 0); }
 
 int bgk_dropin_moments(double* out_dev, void* stream) {
-    if (!g_tracked.on || g_tracked.nparts <= 0 || !g_tracked.partials) return BGK_ERR_STATE;
-    return bgk_dropin_finalize(g_tracked.partials, g_tracked.nparts, out_dev, stream);
+    if (!g_tracked.on || !g_tracked.valid) return BGK_ERR_STATE;
+    const cudaError_t e = cudaMemcpyAsync(out_dev, g_tracked.sums, 5 * sizeof(double), cudaMemcpyDefault,
+                                          (cudaStream_t)stream);
+    return e == cudaSuccess ? BGK_OK : BGK_ERR_CUDA;
 }
+
+const double* bgk_dropin_moments_ptr(void) {
+    return (g_tracked.on && g_tracked.valid) ? g_tracked.sums : nullptr;
+}
+
+void bgk_dropin_moments_to(double* dst) { g_tracked.next = dst; }
 
 }  // extern "C"

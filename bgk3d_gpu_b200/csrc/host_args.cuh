@@ -102,6 +102,8 @@ SweepArgs<S, C> sweep_args(const bgk_sweep_params* p, void* const* a, void* cons
     A.kmin = p->kmin; A.kmax = p->kmax;
     A.mom = nullptr;
     A.mom_span = 8;
+    A.mom_out = nullptr;
+    A.mom_ticket = nullptr;
     A.bcase = p->bcase;
     A.generic = !(p->cte1 == 1.0 && p->cte0 == 0.0 && p->fx == 0.0 && p->fy == 0.0 && p->fz == 0.0);
     A.fast = (p->fast != 0 && sizeof(C) == 4) ? 1 : 0;

@@ -10,7 +10,7 @@
 namespace bgk {
 template <class S, class C>
 int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st,
-                 int* halo = nullptr);
+                 int* halo = nullptr, double* mom_out = nullptr, unsigned* mom_ticket = nullptr);
 template <class S, class C>
 int launch_sweep_tma(const bgk_sweep_params* p, void* const* a, void* const* b, const void* tmap, const int* pa,
                      int* err, cudaStream_t st);
@@ -20,7 +20,8 @@ template <class S, class C>
 int launch_draglift(const bgk_sweep_params* p, void* const* a, int is, int ie, int js, int je, int ks, int ke,
                     double* out, double* ws, size_t ws_bytes, cudaStream_t st);
 template <class S, class C>
-int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st);
+int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st,
+              double* mom_out = nullptr, unsigned* mom_ticket = nullptr);
 template <class S, class C>
 int launch_aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st);
 template <class S, class C>

@@ -66,8 +66,9 @@ void drop_graph(bgk_lattice* L) {
     L->graph_steps = 0;
 }
 
-int aa_step(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st) {
-    KIND_DISPATCH(p->kind, (launch_aa<S, C>(p, slots, odd, mom, st)));
+int aa_step(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st,
+            double* mom_out = nullptr, unsigned* mom_ticket = nullptr) {
+    KIND_DISPATCH(p->kind, (launch_aa<S, C>(p, slots, odd, mom, st, mom_out, mom_ticket)));
 }
 
 int aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
@@ -79,10 +80,14 @@ int aa_prepass(const bgk_sweep_params* p, void* const* slots, cudaStream_t st) {
 // of the new state go to mom (one slot of 5 doubles per block).
 int tma_step(bgk_lattice* L, cudaStream_t st);
 
-int one_step(bgk_lattice* L, cudaStream_t st, double* mom = nullptr) {
+// mom (nullable): per-block moment partials of the new state; mom_out
+// (nullable, with mom): their sums, finalized in the same launch with the
+// ticket counters mom_ticket.
+int one_step(bgk_lattice* L, cudaStream_t st, double* mom = nullptr, double* mom_out = nullptr,
+             unsigned* mom_ticket = nullptr) {
     if (L->desc.pattern == BGK_PATTERN_AA) {
         const bool odd = (L->steps % 2) == 0;   // Layout E -> odd kernel
-        if (int e = aa_step(&L->p, L->a, odd, mom, st)) return e;
+        if (int e = aa_step(&L->p, L->a, odd, mom, st, mom_out, mom_ticket)) return e;
     } else {
         const bool has_obs = L->p.obs && L->p.imin <= L->p.imax;
         if (!mom && L->tma_ok && g_tma_kernels && !has_obs && !L->p.zhalo) {
@@ -90,7 +95,7 @@ int one_step(bgk_lattice* L, cudaStream_t st, double* mom = nullptr) {
             L->outflow_fresh = false;
         } else {
             int halo = L->outflow_fresh ? 1 : 0;
-            if (int e = sweep_launch_mom(&L->p, L->a, L->b, mom, st, &halo)) return e;
+            if (int e = sweep_launch_mom(&L->p, L->a, L->b, mom, st, &halo, mom_out, mom_ticket)) return e;
             L->outflow_fresh = halo != 0;
         }
         for (int d = 0; d < 18; ++d) std::swap(L->a[d], L->b[d]);
@@ -556,20 +561,26 @@ int bgk_lattice_step(bgk_lattice* L, int nsteps, void* stream) {
 int bgk_lattice_step_moments(bgk_lattice* L, int nsteps, int every, double* out_dev, void* stream) {
     if (!L || nsteps < 0 || every < 1 || !out_dev) return set_error(BGK_ERR_ARG, "bad argument");
     cudaStream_t st = (cudaStream_t)stream;
-    const long long nb = sweep_blocks(&L->p, L->a[0], L->desc.pattern == BGK_PATTERN_AB);
-    const size_t need = (size_t)nb * 5 * sizeof(double);
+    // ticket counters and moment records of the launches that sum their own
+    // moments (finalize_by_tickets), laid out for the largest block count
+    // of this lattice's shape; the counters start at zero and every launch
+    // leaves them so
+    const long long nb_max = sweep_blocks(&L->p, nullptr);
+    const size_t need = fused_workspace_bytes(nb_max, 5);
     if (L->mom_bytes < need) {
         dev_free(L->mom);
         L->mom = nullptr; L->mom_bytes = 0;
         if (int rc = dev_alloc(reinterpret_cast<void**>(&L->mom), need, false, "moment partials")) return rc;
         L->mom_bytes = need;
+        cudaError_t e = cudaMemsetAsync(L->mom, 0, need, st);
+        if (e != cudaSuccess) return set_error(BGK_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
     }
+    const FusedWs fw = fused_ws(L->mom, nb_max);
     const int samples = nsteps / every;
     for (int s = 0; s < samples; ++s) {
         if (every > 1)
             if (int e = bgk_lattice_step(L, every - 1, stream)) return e;
-        if (int e = one_step(L, st, L->mom)) return e;
-        if (int e = finalize_moments(L->mom, nb, out_dev + 5 * (size_t)s, st)) return e;
+        if (int e = one_step(L, st, fw.records, out_dev + 5 * (size_t)s, fw.tickets)) return e;
     }
     return bgk_lattice_step(L, nsteps - samples * every, stream);
 }

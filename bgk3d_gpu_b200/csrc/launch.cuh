@@ -121,7 +121,7 @@ template <class S, class C> int coll_mode(const SweepArgs<S, C>& A) {
 // sweeps do not).
 template <class S, class C>
 int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, double* mom, cudaStream_t st,
-                 int* halo) {
+                 int* halo, double* mom_out, unsigned* mom_ticket) {
     SweepArgs<S, C> A = sweep_args<S, C>(p, a, b);
     segment_geometry(A, a[0], true);
     A.mom = mom;
@@ -155,6 +155,9 @@ int launch_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, doub
     const bool obs = A.obs != nullptr;
     const MomPlan mp = mom_plan(warps);
     A.mom_span = (uint32_t)mp.span;
+    if (mom && (!mom_out || !mom_ticket)) return set_error(BGK_ERR_ARG, "moments need their output and counters");
+    A.mom_out = mom_out;
+    A.mom_ticket = mom_ticket;
     const unsigned nb = (unsigned)(mom ? mp.blocks : blocks);
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
         if (g_pair_kernels && mom == nullptr && nelem < (1LL << 31) && pairs_aligned<S>(p, a, b)) {
@@ -401,7 +404,8 @@ void launch_aa_odd_pair(const SweepArgs<S, C>& A, int cm, unsigned blocks, cudaS
 }
 
 template <class S, class C>
-int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st) {
+int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* mom, cudaStream_t st,
+              double* mom_out, unsigned* mom_ticket) {
     SweepArgs<S, C> A = sweep_args<S, C>(p, slots, slots);
     A.b[18] = (S*)slots[18];
     segment_geometry(A, slots[0]);
@@ -410,6 +414,9 @@ int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* m
     if (warps >= (1LL << 32) - 8) return set_error(BGK_ERR_ARG, "lattice too large for one launch");
     const MomPlan mp = mom_plan(warps);
     A.mom_span = (uint32_t)mp.span;
+    if (mom && (!mom_out || !mom_ticket)) return set_error(BGK_ERR_ARG, "moments need their output and counters");
+    A.mom_out = mom_out;
+    A.mom_ticket = mom_ticket;
     const unsigned blocks = (unsigned)(mom ? mp.blocks : (warps + 7) / 8);
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
@@ -593,14 +600,14 @@ int launch_init(void* const* f, long long nx, long long ny, int l, int m, int n,
 #define BGK_INSTANTIATE_AB(S, C)                                                                   \
     namespace bgk {                                                                                \
     template int launch_sweep<S, C>(const bgk_sweep_params*, void* const*, void* const*, double*,  \
-                                    cudaStream_t, int*);                                           \
+                                    cudaStream_t, int*, double*, unsigned*);                       \
     template int launch_sweep_tma<S, C>(const bgk_sweep_params*, void* const*, void* const*,        \
                                         const void*, const int*, int*, cudaStream_t);              \
     }
 #define BGK_INSTANTIATE_AA(S, C)                                                                   \
     namespace bgk {                                                                                \
     template int launch_aa<S, C>(const bgk_sweep_params*, void* const*, bool, double*,             \
-                                 cudaStream_t);                                                    \
+                                 cudaStream_t, double*, unsigned*);                                \
     }
 #define BGK_INSTANTIATE_BATCH(S, C)                                                                \
     namespace bgk {                                                                                \

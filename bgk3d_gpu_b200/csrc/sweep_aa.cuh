@@ -100,6 +100,7 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(co
         for (uint32_t gw = r.beg + (threadIdx.x >> 5); gw < r.end; gw += 8u)
             aa_even_node<S, C, BC, IDX, CM, OBS, true>(P, gw, m5);
         block_reduce_store<5>(m5, P.mom);
+        finalize_by_tickets<5>(P.mom, P.mom_out, P.mom_ticket);
     }
 }
 
@@ -255,6 +256,7 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(con
         for (uint32_t gw = r.beg + (threadIdx.x >> 5); gw < r.end; gw += 8u)
             aa_odd_node<S, C, BC, IDX, CM, OBS, true>(P, gw, m5);
         block_reduce_store<5>(m5, P.mom);
+        finalize_by_tickets<5>(P.mom, P.mom_out, P.mom_ticket);
     }
 }
 

@@ -62,8 +62,10 @@ template <class S, class C> struct SweepArgs {
     int flat;
     uint32_t fwpp;         // warps per z plane
     FastDiv div_fw, div_nx;
-    double* mom;           // optional: per-block FP64 partial moments of the new state
+    double* mom;           // optional: per-block FP64 moment records of the new state (finalize_by_tickets)
     uint32_t mom_span;     // with mom: segments per block (mom_plan), a multiple of 8
+    double* mom_out;       // with mom: the launch's finalized sums, mom_out[0..4]
+    unsigned* mom_ticket;  // with mom: the ticket counters
     int bcase;             // BC_* (used by the batched kernel, which dispatches per tile)
     int generic;           // 1 unless the force-free shifted collision applies
     int fast;              // 1: fused-multiply-add collision (float compute only)
@@ -323,9 +325,9 @@ __device__ __forceinline__ void sweep_at(const SweepArgs<S, C>& P, int i, int j,
 }
 
 // One launch = one time step.  MOM (the launch has P.mom set and the grid of
-// mom_plan, each block advancing one contiguous run of segments): every
-// block also writes the FP64 sums of SRC/diagno.F90's per-node moments of
-// the state it produced (fluid nodes) to P.mom[blockIdx.x * 5 ..].  The two
+// mom_plan, each block advancing one contiguous run of segments): the launch
+// also sums SRC/diagno.F90's per-node moments of the state it produced
+// (fluid nodes) in FP64 into P.mom_out[0..4] (finalize_by_tickets).  The two
 // forms are separate kernels: as one kernel with a run-time branch, changes
 // to either path moved the other's speed by up to 9 % (code layout).
 template <class S, class C, int BC, class IDX, int CM, bool OBS, bool FLAT, bool MOM>
@@ -340,6 +342,7 @@ __global__ void __launch_bounds__(256, (SweepBlocks<S, C>::value)) sweep_ab_kern
         for (uint32_t gw = r.beg + (threadIdx.x >> 5); gw < r.end; gw += 8u)
             sweep_node<S, C, BC, IDX, CM, OBS, FLAT, true>(P, gw, m5);
         block_reduce_store<5>(m5, P.mom);
+        finalize_by_tickets<5>(P.mom, P.mom_out, P.mom_ticket);
     }
 }
 

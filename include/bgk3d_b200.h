@@ -100,10 +100,13 @@ void bgk_sweep_params_init(bgk_sweep_params* p, int kind, int l, int m, int n, d
    outflow halo plane a[9..13](l+1, 1..m, 1..n). */
 int bgk_sweep(const bgk_sweep_params* p, void* const* a, void* const* b, void* stream);
 
-/* bgk_sweep plus, in the same pass, the FP64 moments of the state it writes
-   (the sums bgk_moments would return on that state, up to FP64 summation
-   order) into out_dev[0..4].  Workspace: bgk_sweep_moments_workspace_bytes(p)
-   bytes of device memory (per-block partial sums). */
+/* bgk_sweep plus, in the same launch, the FP64 moments of the state it
+   writes (the sums bgk_moments would return on that state, up to FP64
+   summation order; the same bits on every run) into out_dev[0..4].
+   Workspace: bgk_sweep_moments_workspace_bytes(p) bytes of device memory,
+   no initialisation needed (per-block partial sums and the counters of
+   their in-launch summation, which the call clears first); one workspace
+   per stream of calls. */
 size_t bgk_sweep_moments_workspace_bytes(const bgk_sweep_params* p);
 int bgk_sweep_moments(const bgk_sweep_params* p, void* const* a, void* const* b, double* out_dev,
                       void* workspace, size_t workspace_bytes, void* stream);
@@ -191,11 +194,18 @@ int bgk_probe(const bgk_sweep_params* p, void* const* a, int i, int j, int k, do
 int bgk_slice(const bgk_sweep_params* p, void* const* a, int plane, int index, float* out_dev, void* stream);
 
 /* Helpers of the drop-in library's tracked moments (bgk3d_dropin.h):
-   bgk_sweep with per-block partial moments into partials (when they fit;
-   *nparts = number of partials written, 0 if not), and their second pass. */
-int bgk_dropin_sweep_tracked(const bgk_sweep_params* p, void* const* a, void* const* b, double* partials,
-                             size_t bytes, long long* nparts);
-int bgk_dropin_finalize(const double* partials, long long nparts, double* out_dev, void* stream);
+   bgk_dropin_sweep_tracked is bgk_sweep that also sums, in the same launch,
+   the FP64 moments of the state it writes (rho, u_x, u_y, u_z, 0.5|u|^2 over
+   the fluid nodes, the per-node arithmetic of SRC/diagno.F90:112-127) into
+   out_dev[0..4]: the blocks' partial sums are added in a fixed order by the
+   last blocks to finish, so the bits do not depend on timing.  workspace:
+   bgk_dropin_tracked_workspace_bytes(p) bytes of device memory, zeroed once
+   before its first use with p's lattice shape (it holds counters that every
+   completed call leaves at zero); one workspace per stream of calls.
+   Returns BGK_ERR_ARG when the workspace is too small. */
+size_t bgk_dropin_tracked_workspace_bytes(const bgk_sweep_params* p);
+int bgk_dropin_sweep_tracked(const bgk_sweep_params* p, void* const* a, void* const* b, void* workspace,
+                             size_t bytes, double* out_dev);
 
 /* cudaDeviceSynchronize; returns BGK_ERR_CUDA (does not abort) on failure. */
 int bgk_device_sync(void);

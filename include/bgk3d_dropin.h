@@ -67,12 +67,24 @@ void bgk_dropin_reset(void);
 
 /* Not in the reference: with tracking on, every col_mc_gpu also sums the
    FP64 moments of the state it writes (rho, u_x, u_y, u_z, 0.5|u|^2 over
-   the fluid nodes, the per-node arithmetic of SRC/diagno.F90), in the same pass;
-   bgk_dropin_moments then writes the last call's sums to out_dev[0..4]
-   (device memory) without reading the lattice again.  Returns 0, or
-   BGK_ERR_STATE (-5) when no tracked step exists. */
+   the fluid nodes, the per-node arithmetic of SRC/diagno.F90), in the same
+   launch; bgk_dropin_moments then copies the last call's sums to
+   out_dev[0..4] (device memory, stream-ordered on `stream`) without reading
+   the lattice again.  Returns 0, or BGK_ERR_STATE (-5) when the last
+   col_mc_gpu was not a tracked step.  bgk_dropin_moments_ptr gives the
+   device address of those five sums instead (NULL when there are none):
+   they stay there until the next tracked col_mc_gpu of the calling thread,
+   so a copy from it enqueued on the default stream before that call reads
+   this step's values.  bgk_dropin_moments_to(dst) makes the next tracked
+   col_mc_gpu of the calling thread write its five sums to dst[0..4]
+   instead: device memory, or page-locked host memory (cudaHostAlloc /
+   cudaMallocHost), which the launch writes directly, so a host-side series
+   of per-step sums needs no copy at all (read it after the step completes);
+   bgk_dropin_moments_ptr then returns dst. */
 void bgk_dropin_track_moments(int on);
 int bgk_dropin_moments(double* out_dev, void* stream);
+const double* bgk_dropin_moments_ptr(void);
+void bgk_dropin_moments_to(double* dst);
 
 #ifdef __cplusplus
 }
