@@ -16,7 +16,8 @@ from _cases import BCASE, CASE_PARAMS, OMEGA, SCALE, interior, random_state
 pytestmark = pytest.mark.gpu
 
 CASES = ["driven", "periodic", "channel", "channel_const", "inflow", "none"]
-SHAPES = [(70, 13, 9), (128, 12, 6), (33, 22, 5), (200, 5, 4), (2, 6, 4), (64, 5, 4), (66, 4, 3)]
+SHAPES = [(70, 13, 9), (128, 12, 6), (33, 22, 5), (200, 5, 4), (2, 6, 4), (64, 5, 4), (66, 4, 3), (150, 6, 4),
+          (290, 4, 3)]
 
 
 def _switch(on: bool) -> int:
