@@ -389,17 +389,33 @@ void launch_aa_bc(const SweepArgs<S, C>& A, bool odd, long long nelem, unsigned 
     else by_variant<AaEvenLaunch, S, C, BC>(nelem, cm, obs, A, blocks, st);
 }
 
+template <class S, class C, int BC, bool OBS>
+void launch_aa_odd_pair_obs(const SweepArgs<S, C>& A, int cm, unsigned blocks, cudaStream_t st) {
+    switch (cm) {
+        case CM_STRICT: aa_odd_pair_kernel<S, C, BC, CM_STRICT, OBS><<<blocks, kPairThreads, 0, st>>>(A); break;
+        case CM_STRICT_GENERIC:
+            aa_odd_pair_kernel<S, C, BC, CM_STRICT_GENERIC, OBS><<<blocks, kPairThreads, 0, st>>>(A);
+            break;
+        case CM_FAST: aa_odd_pair_kernel<S, C, BC, CM_FAST, OBS><<<blocks, kPairThreads, 0, st>>>(A); break;
+        default: aa_odd_pair_kernel<S, C, BC, CM_FAST_GENERIC, OBS><<<blocks, kPairThreads, 0, st>>>(A); break;
+    }
+}
 template <class S, class C, int BC>
-void launch_aa_odd_pair(const SweepArgs<S, C>& A, int cm, unsigned blocks, cudaStream_t st) {
+void launch_aa_odd_pair(const SweepArgs<S, C>& A, int cm, bool obs, unsigned blocks, cudaStream_t st) {
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
-        switch (cm) {
-            case CM_STRICT: aa_odd_pair_kernel<S, C, BC, CM_STRICT><<<blocks, kPairThreads, 0, st>>>(A); break;
-            case CM_STRICT_GENERIC:
-                aa_odd_pair_kernel<S, C, BC, CM_STRICT_GENERIC><<<blocks, kPairThreads, 0, st>>>(A);
-                break;
-            case CM_FAST: aa_odd_pair_kernel<S, C, BC, CM_FAST><<<blocks, kPairThreads, 0, st>>>(A); break;
-            default: aa_odd_pair_kernel<S, C, BC, CM_FAST_GENERIC><<<blocks, kPairThreads, 0, st>>>(A); break;
-        }
+        if (obs) launch_aa_odd_pair_obs<S, C, BC, true>(A, cm, blocks, st);
+        else launch_aa_odd_pair_obs<S, C, BC, false>(A, cm, blocks, st);
+    }
+}
+template <class S, class C, bool INFLOW, bool OBS>
+void launch_aa_even_pair(const SweepArgs<S, C>& A, int cm, unsigned blocks, cudaStream_t st) {
+    switch (cm) {
+        case CM_STRICT: aa_even_pair_kernel<S, C, CM_STRICT, INFLOW, OBS><<<blocks, kPairThreads, 0, st>>>(A); break;
+        case CM_STRICT_GENERIC:
+            aa_even_pair_kernel<S, C, CM_STRICT_GENERIC, INFLOW, OBS><<<blocks, kPairThreads, 0, st>>>(A);
+            break;
+        case CM_FAST: aa_even_pair_kernel<S, C, CM_FAST, INFLOW, OBS><<<blocks, kPairThreads, 0, st>>>(A); break;
+        default: aa_even_pair_kernel<S, C, CM_FAST_GENERIC, INFLOW, OBS><<<blocks, kPairThreads, 0, st>>>(A); break;
     }
 }
 
@@ -421,28 +437,29 @@ int launch_aa(const bgk_sweep_params* p, void* const* slots, bool odd, double* m
     const long long nelem = p->nx * p->ny * ((long long)p->n + 2) + 64;
     if constexpr (sizeof(S) == 2 && sizeof(C) == 4) {
         const int cm = coll_mode(A);
-        if (g_pair_kernels && A.obs == nullptr && mom == nullptr && p->bcase != BC_INFLOW &&
-            nelem < (1LL << 31) && pairs_aligned<S>(p, slots, slots)) {
+        if (g_pair_kernels && mom == nullptr && p->bcase != BC_NONE && nelem < (1LL << 31) &&
+            pairs_aligned<S>(p, slots, slots)) {
             SweepArgs<S, C> A2 = A;
             A2.nseg = (p->l + 63) / 64;
             A2.div_seg.init((uint32_t)A2.nseg);
             constexpr int wpb = kPairThreads / 32;
             const unsigned nb2 = (unsigned)(((long long)A2.nseg * p->m * p->n + wpb - 1) / wpb);
+            const bool obs = A.obs != nullptr, inflow = p->bcase == BC_INFLOW;
             if (!odd) {
-                switch (cm) {
-                    case CM_STRICT: aa_even_pair_kernel<S, C, CM_STRICT><<<nb2, kPairThreads, 0, st>>>(A2); break;
-                    case CM_STRICT_GENERIC:
-                        aa_even_pair_kernel<S, C, CM_STRICT_GENERIC><<<nb2, kPairThreads, 0, st>>>(A2);
-                        break;
-                    case CM_FAST: aa_even_pair_kernel<S, C, CM_FAST><<<nb2, kPairThreads, 0, st>>>(A2); break;
-                    default: aa_even_pair_kernel<S, C, CM_FAST_GENERIC><<<nb2, kPairThreads, 0, st>>>(A2); break;
+                if (inflow) {
+                    if (obs) launch_aa_even_pair<S, C, true, true>(A2, cm, nb2, st);
+                    else launch_aa_even_pair<S, C, true, false>(A2, cm, nb2, st);
+                } else {
+                    if (obs) launch_aa_even_pair<S, C, false, true>(A2, cm, nb2, st);
+                    else launch_aa_even_pair<S, C, false, false>(A2, cm, nb2, st);
                 }
                 return check_launch("aa_even_pair_kernel");
             }
             switch (p->bcase) {
-                case BC_DRIVEN: launch_aa_odd_pair<S, C, BC_DRIVEN>(A2, cm, nb2, st); break;
-                case BC_PERIODIC: launch_aa_odd_pair<S, C, BC_PERIODIC>(A2, cm, nb2, st); break;
-                case BC_CHANNEL: launch_aa_odd_pair<S, C, BC_CHANNEL>(A2, cm, nb2, st); break;
+                case BC_DRIVEN: launch_aa_odd_pair<S, C, BC_DRIVEN>(A2, cm, obs, nb2, st); break;
+                case BC_PERIODIC: launch_aa_odd_pair<S, C, BC_PERIODIC>(A2, cm, obs, nb2, st); break;
+                case BC_CHANNEL: launch_aa_odd_pair<S, C, BC_CHANNEL>(A2, cm, obs, nb2, st); break;
+                case BC_INFLOW: launch_aa_odd_pair<S, C, BC_INFLOW>(A2, cm, obs, nb2, st); break;
                 default: return set_error(BGK_ERR_ARG, "AA lattices need a boundary case");
             }
             return check_launch("aa_odd_pair_kernel");

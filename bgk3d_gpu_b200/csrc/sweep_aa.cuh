@@ -50,13 +50,10 @@ __device__ __forceinline__ bool aa_node(const SweepArgs<S, C>& P, uint32_t gw, i
     return true;
 }
 
-// Even (local) step.  P.a and P.b both name the slot arrays.  Arithmetic in
-// storage units, as in sweep_node.
+// Even (local) step of node (i, j, k) at element c.  P.a and P.b both name
+// the slot arrays.  Arithmetic in storage units, as in sweep_node.
 template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
-__device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
-    int i, j, k;
-    IDX c;
-    if (!aa_node<S, C, IDX>(P, gw, i, j, k, c)) return;
+__device__ __forceinline__ void aa_even_at(const SweepArgs<S, C>& P, int i, int j, int k, IDX c, double (&m5)[5]) {
     if (OBS && P.obs != nullptr && i >= P.imin && i <= P.imax && j >= P.jmin && j <= P.jmax &&
         k >= P.kmin && k <= P.kmax && (obstacle_links(P, i, j, k) & 0x80000000u))
         return;
@@ -90,6 +87,15 @@ __device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, uint32_t 
     }
 }
 
+// Even step of this lane's node.
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
+__device__ __forceinline__ void aa_even_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
+    int i, j, k;
+    IDX c;
+    if (!aa_node<S, C, IDX>(P, gw, i, j, k, c)) return;
+    aa_even_at<S, C, BC, IDX, CM, OBS, MOM>(P, i, j, k, c, m5);
+}
+
 template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -109,10 +115,12 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_even_kernel(co
 // words of its pair (i, i + 1), runs the two collisions as one on packed
 // FP32 pairs and writes population p of both nodes as one word into slot
 // opp(p); bit-identical to aa_even_kernel, in either collision mode.  Purely
-// local, so no shuffles.
-// No obstacle, no fused moments, not the inflow case (whose node l also
-// writes the outflow halo); the host takes aa_even_kernel for those.
-template <class S, class C, int CM>
+// local, so no shuffles.  INFLOW: node l also writes the outflow halo
+// (aa_even_at's rule) from its values just stored.  OBS: a warp whose 64
+// nodes touch the obstacle's box grown by one node advances them node by
+// node with the one-node rules (solid nodes are not updated).  No fused
+// moments.
+template <class S, class C, int CM, bool INFLOW, bool OBS>
 __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel(const SweepArgs<S, C> P) {
     static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair step: 16-bit storage, float compute");
     const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
@@ -126,6 +134,13 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel
     const int i0 = seg * 64 + 2 * lane + 1;
     if (i0 >= P.l) return;                            // l even: the pair (i0, i0 + 1) is inside
     const int c = (int)P.nx * j + (int)P.nxy * k + i0;
+    if (OBS && P.obs != nullptr && j >= P.jmin - 1 && j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1 &&
+        seg * 64 + 64 >= P.imin - 1 && seg * 64 + 1 <= P.imax + 1) {
+        double m5[5];
+        aa_even_at<S, C, INFLOW ? BC_INFLOW : BC_NONE, int, CM, true, false>(P, i0, j, k, c, m5);
+        aa_even_at<S, C, INFLOW ? BC_INFLOW : BC_NONE, int, CM, true, false>(P, i0 + 1, j, k, c + 1, m5);
+        return;
+    }
     // P.a and P.b name the same slot arrays (P.b[18] too)
     uint32_t wv[19];
 #pragma unroll
@@ -137,15 +152,25 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel
         bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
     else
         bgk_collide_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.col, P.inv_scale);
+    if (INFLOW && i0 + 1 == P.l) {
+        // node l is the high half: its populations as just stored (slot
+        // opp(d), this thread's own stores), the outflow equilibria into the
+        // halo cell l + 1, as aa_even_at writes them
+        const int cl = c + 1;
+        C r[19];
+#pragma unroll
+        for (int d = 0; d < 19; ++d) r[d] = Conv<S, C>::raw(P.b[opp_of(d)][cl]);
+        C eq[5];
+        outflow_eq<C, Scaled<S>::value>(r, P.inflow_cte1, P.col, P.inv_scale, eq);
+#pragma unroll
+        for (int e = 0; e < 5; ++e) P.b[opp_of(9 + e)][cl + 1] = Conv<S, C>::pack(eq[e]);
+    }
 }
 
-// Odd (pull + push) step.
+// Odd (pull + push) step of node (i, j, k) at element c.
 template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
-__device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
+__device__ __forceinline__ void aa_odd_at(const SweepArgs<S, C>& P, int i, int j, int k, IDX c, double (&m5)[5]) {
     typedef Faces<BC> F;
-    int i, j, k;
-    IDX c;
-    if (!aa_node<S, C, IDX>(P, gw, i, j, k, c)) return;
     uint32_t sl = 0;
     if (OBS && P.obs != nullptr && i >= P.imin - 1 && i <= P.imax + 1 && j >= P.jmin - 1 &&
         j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1) {
@@ -246,6 +271,15 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t g
     }
 }
 
+// Odd step of this lane's node.
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
+__device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t gw, double (&m5)[5]) {
+    int i, j, k;
+    IDX c;
+    if (!aa_node<S, C, IDX>(P, gw, i, j, k, c)) return;
+    aa_odd_at<S, C, BC, IDX, CM, OBS, MOM>(P, i, j, k, c, m5);
+}
+
 template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
 __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(const SweepArgs<S, C> P) {
     double m5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -261,8 +295,12 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(con
 }
 
 // Odd step of the 16-bit kinds on aligned pairs (the layout of
-// aa_even_pair_kernel; driven cavity, periodic and channel cases; no
-// obstacle, no fused moments).  Pull: population d of the pair's nodes comes
+// aa_even_pair_kernel; every boundary case; no fused moments).  Inflow:
+// node 1 pulls the inflow equilibrium across x = 0 and writes it into its
+// own slots 01..05, its populations leaving through x = 0 are dropped, and
+// node l writes the outflow equilibria of its new state (aa_odd_at's rules).
+// OBS: a warp whose 64 nodes touch the obstacle's box grown by one node
+// advances them node by node with the one-node rules.  Pull: population d of the pair's nodes comes
 // from slot opp(d) of the source row as one 32-bit word, the x-shifted half
 // through a lane shuffle as in sweep_abp_kernel (behind a wall: own slot d).
 // Push: population d of both nodes goes to slot d of the target row; for
@@ -273,10 +311,11 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(con
 // read it (or, within a warp, after the neighbour lane's read through the
 // shuffled data), so the in-place update has no hazard.  Bit-identical to
 // aa_odd_kernel.
-template <class S, class C, int BC, int CM>
+template <class S, class C, int BC, int CM, bool OBS>
 __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(const SweepArgs<S, C> P) {
     static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair step: 16-bit storage, float compute");
-    static_assert(BC == BC_DRIVEN || BC == BC_PERIODIC || BC == BC_CHANNEL, "pair odd step: no inflow");
+    static_assert(BC == BC_DRIVEN || BC == BC_PERIODIC || BC == BC_CHANNEL || BC == BC_INFLOW,
+                  "pair odd step: a boundary case");
     typedef Faces<BC> F;
     const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -291,6 +330,18 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(
     const int ia = valid ? i0 : P.l - 1;              // other lanes read a valid pair, store nothing
     const int nx = (int)P.nx, nxy = (int)P.nxy;
     const int c = nx * j + nxy * k + ia;
+    if (OBS && P.obs != nullptr && j >= P.jmin - 1 && j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1 &&
+        seg * 64 + 64 >= P.imin - 1 && seg * 64 + 1 <= P.imax + 1) {
+        // the warp's 64 nodes touch the obstacle's box grown by one node:
+        // node by node with the one-node rules (each node reads and writes
+        // only slots no other node touches, so the order does not matter)
+        double m5[5];
+        if (valid) {
+            aa_odd_at<S, C, BC, int, CM, true, false>(P, ia, j, k, c, m5);
+            aa_odd_at<S, C, BC, int, CM, true, false>(P, ia + 1, j, k, c + 1, m5);
+        }
+        return;
+    }
     const bool at_lo = ia == 1, at_hi = ia + 1 == P.l;
     const bool edge_lo = lane == 0 || at_lo, edge_hi = lane == 31 || at_hi;
     const int oym = (F::PY && j == 1) ? (P.m - 1) * nx : -nx;
@@ -329,7 +380,8 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(
         uint32_t v = w[d];
         if (cx == 1) {
             const uint32_t left = __shfl_up_sync(0xffffffffu, v, 1) >> 16;
-            const uint32_t lo = edge_lo ? e[d] : left;
+            uint32_t lo = edge_lo ? e[d] : left;
+            if (BC == BC_INFLOW && at_lo) lo = s_bits(P.inflow_s[d]);   // the inflow face x = 0
             if (!wall[d]) v = __byte_perm(lo, v, 0x5410);
         } else if (cx == -1) {
             const uint32_t right = __shfl_down_sync(0xffffffffu, v, 1) & 0xffffu;
@@ -386,7 +438,8 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(
             else st32(d, off, __byte_perm(pk, next_a, 0x5432));
             if (edge_lo) {                                    // node ia -> ia - 1 leaves the lane's word
                 if (at_lo && F::WX) st16(od, c, bounce_bits(od, pk & 0xffffu));
-                else st16(d, off + ((F::PX && at_lo) ? P.l - 1 : -1), pk & 0xffffu);
+                else if (!(BC == BC_INFLOW && at_lo))         // through the inflow face: gone
+                    st16(d, off + ((F::PX && at_lo) ? P.l - 1 : -1), pk & 0xffffu);
             }
         } else {
             if (!valid) return;
@@ -398,6 +451,37 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(
         bgk_collide_fast_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.fc, P.inv_scale);
     else
         bgk_collide_f<F2, float, cm_generic(CM), Scaled<S>::value>(xs, xp, ys, P.col, P.inv_scale);
+    if (BC == BC_INFLOW && valid && at_lo) {
+        // node 1: the inflow equilibrium into its own slots 01..05 (no node
+        // pushes into them), as aa_odd_at writes it
+#pragma unroll
+        for (int d = 0; d < 5; ++d) st16(d, c, s_bits(P.inflow_s[d]));
+    }
+    if (BC == BC_INFLOW && valid && at_hi) {
+        // node l is the high half: its populations where this thread has
+        // just pushed them (c_x = 0: the high half of the target word; c_x =
+        // +1: the halo cell l + 1, which the next even step rewrites; c_x =
+        // -1: node l - 1), then the outflow equilibria into slots 10..14 of
+        // (l, j + c_y, k + c_z), as aa_odd_at writes them
+        auto target = [&](int d) {
+            const int cy = cy_of(d), cz = cz_of(d);
+            int off = c;
+            if (cy == 1) off += oyp; else if (cy == -1) off += oym;
+            if (cz == 1) off += ozp; else if (cz == -1) off += ozm;
+            return off;
+        };
+        C r[19];
+#pragma unroll
+        for (int d = 0; d < 18; ++d) {
+            const int cx = cx_of(d);
+            r[d] = Conv<S, C>::raw(P.b[d][target(d) + (cx == 1 ? 2 : (cx == -1 ? 0 : 1))]);
+        }
+        r[18] = Conv<S, C>::raw(P.b[18][c + 1]);
+        C eq[5];
+        outflow_eq<C, Scaled<S>::value>(r, P.inflow_cte1, P.col, P.inv_scale, eq);
+#pragma unroll
+        for (int e = 0; e < 5; ++e) P.b[9 + e][target(9 + e) + 1] = Conv<S, C>::pack(eq[e]);
+    }
 }
 
 // Outflow halo in slot form for a freshly loaded Layout E state: halo cell

@@ -108,7 +108,7 @@ def main(argv=None) -> int:
                                 path = "tma"
                             elif pair == "on" and BYTES[kind] == 2 and pattern == "ab":
                                 path = "two-node"
-                            elif pair == "on" and BYTES[kind] == 2 and case != "inflow":
+                            elif pair == "on" and BYTES[kind] == 2:
                                 path = "two-node even step"
                             else:
                                 path = "one-node"

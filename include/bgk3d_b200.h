@@ -243,7 +243,7 @@ int bgk_set_obstacle_split(int enable);
    every node pair (i, i + 1), i odd, is one aligned 32-bit word (library-owned
    lattices of even l) the pair is adjacent and each population moves as one
    word, in either collision mode (and both steps of the AA pattern run in
-   pairs, except with an obstacle or the inflow case); otherwise, with the fused collision (fast = 1), the thread takes
+   pairs); otherwise, with the fused collision (fast = 1), the thread takes
    nodes i and i + 32.  Used by bgk_sweep and lattice steps.  On by default;
    0 selects the one-node sweep.  Returns the previous setting (not
    thread-safe against concurrent launches).  No counterpart in the

@@ -65,12 +65,16 @@ def test_aa_interior_warps_match_oracle(kind, pair, case):
     assert_fluid_equal(got, want, fluid, f"aa interior kind={kind} case={case}")
 
 
+@pytest.mark.parametrize("kind", [1, 2, 3])
 @pytest.mark.parametrize("case", ["driven", "periodic", "inflow", "channel"])
-def test_aa_interior_warps_with_obstacle(case):
+def test_aa_interior_warps_with_obstacle(kind, case):
+    """70-node rows with a sphere: FP32 one node per thread; FP16 and BF16
+    through the AA pair steps, whose warps near the sphere fall back to the
+    one-node rules."""
     l, m, n = 70, 9, 8
     obs = sphere_mask(l, m, n, (40.0, 5.0, 4.5), 4.0)
-    got, want, fluid = run_pair(l, m, n, 1, case, "aa", steps=6, seed=31, obs=obs)
-    assert_fluid_equal(got, want, fluid, f"aa interior obstacle case={case}")
+    got, want, fluid = run_pair(l, m, n, kind, case, "aa", steps=6, seed=31, obs=obs)
+    assert_fluid_equal(got, want, fluid, f"aa interior obstacle kind={kind} case={case}")
 
 
 @pytest.mark.parametrize("pattern", ["ab", "aa"])

@@ -11,7 +11,7 @@ import zlib
 import numpy as np
 import pytest
 
-from _cases import BCASE, CASE_PARAMS, OMEGA, SCALE, interior, random_state
+from _cases import BCASE, CASE_PARAMS, OMEGA, SCALE, interior, random_state, sphere_mask
 
 pytestmark = pytest.mark.gpu
 
@@ -25,7 +25,7 @@ def _switch(on: bool) -> int:
     return lib().bgk_set_pair_kernels(1 if on else 0)
 
 
-def _lattice(kind, case, shape, fast, on, steps=5, pattern="ab"):
+def _lattice(kind, case, shape, fast, on, steps=5, pattern="ab", obs=None):
     from bgk3d_gpu_b200.lattice import Lattice
     l, m, n = shape
     p = CASE_PARAMS[case]
@@ -34,6 +34,8 @@ def _lattice(kind, case, shape, fast, on, steps=5, pattern="ab"):
         lat = Lattice(l, m, n, kind=kind, bcase=BCASE[case], omega=OMEGA, scale=SCALE[kind], fast=fast,
                       pattern=pattern, lid_force=p.get("lid_force", 0.0), u_inflow=p.get("u_inflow", 0.0),
                       force_mode=p.get("force_mode", 0), force=p.get("force", (0.0, 0.0, 0.0)))
+        if obs is not None:
+            lat.set_obstacle(obs)
         seed = zlib.crc32(repr((kind, case, shape)).encode()) % 1000
         lat.upload(random_state(l, m, n, kind, seed=seed, scale=SCALE[kind]))
         lat.step(steps)
@@ -86,8 +88,10 @@ def test_pair_equals_one_node_sweep_on_reference_layout(kind, case, ipad, jpad):
 @pytest.mark.parametrize("case", [c for c in CASES if c != "none"])
 @pytest.mark.parametrize("fast", [False, True])
 def test_aa_even_pair_step_equals_one_node_step(kind, case, fast):
-    """The in-place pattern: even steps through aa_even_pair_kernel, odd steps
-    through aa_odd_kernel, against both through the one-node kernels."""
+    """The in-place pattern: both steps through the pair kernels
+    (aa_even_pair_kernel, aa_odd_pair_kernel; for the inflow case with the
+    inflow face, node 1's own inflow slots and node l's outflow equilibria),
+    against both through the one-node kernels."""
     for shape in SHAPES:
         a = _lattice(kind, case, shape, fast, True, steps=6, pattern="aa")
         b = _lattice(kind, case, shape, fast, False, steps=6, pattern="aa")
@@ -128,3 +132,20 @@ def test_pair_switch_default_on():
     prev = _switch(True)
     assert _switch(bool(prev)) == 1
     assert prev == 1
+
+
+@pytest.mark.parametrize("kind", [2, 3])
+@pytest.mark.parametrize("case", [c for c in CASES if c != "none"])
+@pytest.mark.parametrize("fast", [False, True])
+def test_aa_pair_steps_with_obstacle_equal_one_node_steps(kind, case, fast):
+    """The in-place pattern with a sphere: the pair steps' warps that touch
+    the obstacle's grown box advance their nodes one by one with the one-node
+    rules, the others in pairs; every node (solid ones stay as uploaded)
+    against the one-node kernels."""
+    for shape in [(70, 13, 9), (128, 12, 10), (150, 9, 8)]:
+        l, m, n = shape
+        obs = sphere_mask(l, m, n, (l / 2, (m + 1) / 2, (n + 1) / 2), min(m, n) / 2)
+        a = _lattice(kind, case, shape, fast, True, steps=6, pattern="aa", obs=obs)
+        b = _lattice(kind, case, shape, fast, False, steps=6, pattern="aa", obs=obs)
+        bad = np.argwhere(a != b)
+        assert len(bad) == 0, (kind, case, shape, len(bad), bad[:5].tolist())
