@@ -167,8 +167,10 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_even_pair_kernel
     }
 }
 
-// Odd (pull + push) step of node (i, j, k) at element c.
-template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
+// Odd (pull + push) step of node (i, j, k) at element c.  YZW = false: the
+// node's row lies on no y or z wall (and so not on the driven lid); that
+// logic is compiled out.
+template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM, bool YZW = true>
 __device__ __forceinline__ void aa_odd_at(const SweepArgs<S, C>& P, int i, int j, int k, IDX c, double (&m5)[5]) {
     typedef Faces<BC> F;
     uint32_t sl = 0;
@@ -189,8 +191,8 @@ __device__ __forceinline__ void aa_odd_at(const SweepArgs<S, C>& P, int i, int j
     const IDX ozp = (F::PZ && k == P.n) ? (IDX)(1 - P.n) * nxy : nxy;
     // the -1 / +1 neighbour lies behind a wall
     const bool wxm = F::WX && i == 1, wxp = F::WX && i == P.l;
-    const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
-    const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
+    const bool wym = YZW && F::WY && j == 1, wyp = YZW && F::WY && j == P.m;
+    const bool wzm = YZW && F::WZ && k == 1, wzp = YZW && F::WZ && k == P.n;
     const float inv = P.inv_scale;
     C x[19];
 #pragma unroll
@@ -206,7 +208,7 @@ __device__ __forceinline__ void aa_odd_at(const SweepArgs<S, C>& P, int i, int j
         if (cy == 1) bounce |= wym; else if (cy == -1) bounce |= wyp;
         if (cz == 1) bounce |= wzm; else if (cz == -1) bounce |= wzp;
         C v = Conv<S, C>::raw(bounce ? P.a[d][c] : P.a[opp_of(d)][off]);
-        if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
+        if (YZW && BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n)
             v = roundtrip<S, C>(d == 1 ? v + P.lid_force : v - P.lid_force);
         if (BC == BC_INFLOW && cx == 1 && i == 1)
             v = Conv<S, C>::raw(P.inflow_s[d]);
@@ -232,7 +234,7 @@ __device__ __forceinline__ void aa_odd_at(const SweepArgs<S, C>& P, int i, int j
         if (cz == 1) bounce |= wzp; else if (cz == -1) bounce |= wzm;
         if (bounce) {
             S bv = sv[d];
-            if (BC == BC_DRIVEN && (od == 1 || od == 10) && k == P.n) {
+            if (YZW && BC == BC_DRIVEN && (od == 1 || od == 10) && k == P.n) {
                 const C r = Conv<S, C>::raw(sv[d]);
                 bv = Conv<S, C>::pack(od == 1 ? r + P.lid_force : r - P.lid_force);
             }
@@ -277,7 +279,12 @@ __device__ __forceinline__ void aa_odd_node(const SweepArgs<S, C>& P, uint32_t g
     int i, j, k;
     IDX c;
     if (!aa_node<S, C, IDX>(P, gw, i, j, k, c)) return;
-    aa_odd_at<S, C, BC, IDX, CM, OBS, MOM>(P, i, j, k, c, m5);
+    // the driven cavity's rows inside its y and z walls (the same for the
+    // whole warp) run without the wall and lid logic
+    if (BC == BC_DRIVEN && j > 1 && j < P.m && k > 1 && k < P.n)
+        aa_odd_at<S, C, BC, IDX, CM, OBS, MOM, false>(P, i, j, k, c, m5);
+    else
+        aa_odd_at<S, C, BC, IDX, CM, OBS, MOM, true>(P, i, j, k, c, m5);
 }
 
 template <class S, class C, int BC, class IDX, int CM, bool OBS, bool MOM>
