@@ -301,62 +301,22 @@ __global__ void __launch_bounds__(256, sizeof(C) == 8 ? 3 : 4) aa_odd_kernel(con
     }
 }
 
-// Odd step of the 16-bit kinds on aligned pairs (the layout of
-// aa_even_pair_kernel; every boundary case; no fused moments).  Inflow:
-// node 1 pulls the inflow equilibrium across x = 0 and writes it into its
-// own slots 01..05, its populations leaving through x = 0 are dropped, and
-// node l writes the outflow equilibria of its new state (aa_odd_at's rules).
-// OBS: a warp whose 64 nodes touch the obstacle's box grown by one node
-// advances them node by node with the one-node rules.  Pull: population d of the pair's nodes comes
-// from slot opp(d) of the source row as one 32-bit word, the x-shifted half
-// through a lane shuffle as in sweep_abp_kernel (behind a wall: own slot d).
-// Push: population d of both nodes goes to slot d of the target row; for
-// c_x = +-1 the word at the lane's own pair position holds one value of this
-// lane and one of its neighbour lane (a shuffle), and the value that leaves
-// the warp (or crosses an x face: wrap, bounce-back into own slot opp(d))
-// is stored as a 16-bit value.  Every slot is written once, by the node that
-// read it (or, within a warp, after the neighbour lane's read through the
-// shuffled data), so the in-place update has no hazard.  Bit-identical to
-// aa_odd_kernel.
-template <class S, class C, int BC, int CM, bool OBS>
-__global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(const SweepArgs<S, C> P) {
-    static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair step: 16-bit storage, float compute");
-    static_assert(BC == BC_DRIVEN || BC == BC_PERIODIC || BC == BC_CHANNEL || BC == BC_INFLOW,
-                  "pair odd step: a boundary case");
+// The pairs of one warp of aa_odd_pair_kernel in row (j, k), lane's pair at
+// node ia (element c).  WALLS = false: the row lies on no y or z wall (the
+// driven cavity's inner rows), whose tests and lid term are compiled out.
+template <class S, class C, int BC, int CM, bool WALLS>
+__device__ __forceinline__ void aa_odd_pair_row(const SweepArgs<S, C>& P, int j, int k, int lane, int ia, bool valid,
+                                                int c) {
     typedef Faces<BC> F;
-    const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    const uint32_t row = P.div_seg.div(gw);
-    if (row >= P.nrows) return;                       // whole warp
-    const int seg = (int)(gw - row * (uint32_t)P.nseg);
-    const uint32_t kk = P.div_m.div(row);
-    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
-    const int k = (int)kk + 1;
-    const int i0 = seg * 64 + 2 * lane + 1;
-    const bool valid = i0 < P.l;                      // l even: the pair (i0, i0 + 1) is inside
-    const int ia = valid ? i0 : P.l - 1;              // other lanes read a valid pair, store nothing
     const int nx = (int)P.nx, nxy = (int)P.nxy;
-    const int c = nx * j + nxy * k + ia;
-    if (OBS && P.obs != nullptr && j >= P.jmin - 1 && j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1 &&
-        seg * 64 + 64 >= P.imin - 1 && seg * 64 + 1 <= P.imax + 1) {
-        // the warp's 64 nodes touch the obstacle's box grown by one node:
-        // node by node with the one-node rules (each node reads and writes
-        // only slots no other node touches, so the order does not matter)
-        double m5[5];
-        if (valid) {
-            aa_odd_at<S, C, BC, int, CM, true, false>(P, ia, j, k, c, m5);
-            aa_odd_at<S, C, BC, int, CM, true, false>(P, ia + 1, j, k, c + 1, m5);
-        }
-        return;
-    }
     const bool at_lo = ia == 1, at_hi = ia + 1 == P.l;
     const bool edge_lo = lane == 0 || at_lo, edge_hi = lane == 31 || at_hi;
     const int oym = (F::PY && j == 1) ? (P.m - 1) * nx : -nx;
     const int oyp = (F::PY && j == P.m) ? (1 - P.m) * nx : nx;
     const int ozm = (F::PZ && k == 1) ? (P.n - 1) * nxy : -nxy;
     const int ozp = (F::PZ && k == P.n) ? (1 - P.n) * nxy : nxy;
-    const bool wym = F::WY && j == 1, wyp = F::WY && j == P.m;
-    const bool wzm = F::WZ && k == 1, wzp = F::WZ && k == P.n;
+    const bool wym = WALLS && F::WY && j == 1, wyp = WALLS && F::WY && j == P.m;
+    const bool wzm = WALLS && F::WZ && k == 1, wzp = WALLS && F::WZ && k == P.n;
     // ---- pull (all loads first)
     uint32_t w[18], e[18];
     bool wall[18];
@@ -395,7 +355,7 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(
             const uint32_t hi = edge_hi ? e[d] : right;
             if (!wall[d]) v = __byte_perm(v, hi, 0x5432);
         }
-        if (BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n) {
+        if (WALLS && BC == BC_DRIVEN && (d == 1 || d == 10) && k == P.n) {
             F2 f = raw_bits<S>(v);
             f.v.x = roundtrip<S, C>(d == 1 ? f.v.x + P.lid_force : f.v.x - P.lid_force);
             f.v.y = roundtrip<S, C>(d == 1 ? f.v.y + P.lid_force : f.v.y - P.lid_force);
@@ -406,7 +366,7 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(
     wv[18] = *reinterpret_cast<const unsigned*>(P.a[18] + c);
     // ---- collision, and the push of each population as soon as it is known
     auto bounce_bits = [&](int od, uint32_t bits) -> uint32_t {   // lid on a wall-reflected value
-        if (BC == BC_DRIVEN && (od == 1 || od == 10) && k == P.n) {
+        if (WALLS && BC == BC_DRIVEN && (od == 1 || od == 10) && k == P.n) {
             const C r = Conv<S, C>::raw(bits_s<S>(bits));
             return s_bits(Conv<S, C>::pack(od == 1 ? r + P.lid_force : r - P.lid_force));
         }
@@ -489,6 +449,60 @@ __global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(
 #pragma unroll
         for (int e = 0; e < 5; ++e) P.b[9 + e][target(9 + e) + 1] = Conv<S, C>::pack(eq[e]);
     }
+}
+
+// Odd step of the 16-bit kinds on aligned pairs (the layout of
+// aa_even_pair_kernel; every boundary case; no fused moments).  Inflow:
+// node 1 pulls the inflow equilibrium across x = 0 and writes it into its
+// own slots 01..05, its populations leaving through x = 0 are dropped, and
+// node l writes the outflow equilibria of its new state (aa_odd_at's rules).
+// OBS: a warp whose 64 nodes touch the obstacle's box grown by one node
+// advances them node by node with the one-node rules.  Pull: population d of the pair's nodes comes
+// from slot opp(d) of the source row as one 32-bit word, the x-shifted half
+// through a lane shuffle as in sweep_abp_kernel (behind a wall: own slot d).
+// Push: population d of both nodes goes to slot d of the target row; for
+// c_x = +-1 the word at the lane's own pair position holds one value of this
+// lane and one of its neighbour lane (a shuffle), and the value that leaves
+// the warp (or crosses an x face: wrap, bounce-back into own slot opp(d))
+// is stored as a 16-bit value.  Every slot is written once, by the node that
+// read it (or, within a warp, after the neighbour lane's read through the
+// shuffled data), so the in-place update has no hazard.  Bit-identical to
+// aa_odd_kernel.
+template <class S, class C, int BC, int CM, bool OBS>
+__global__ void __launch_bounds__(kPairThreads, kPairBlocks) aa_odd_pair_kernel(const SweepArgs<S, C> P) {
+    static_assert(sizeof(S) == 2 && sizeof(C) == 4, "pair step: 16-bit storage, float compute");
+    static_assert(BC == BC_DRIVEN || BC == BC_PERIODIC || BC == BC_CHANNEL || BC == BC_INFLOW,
+                  "pair odd step: a boundary case");
+    typedef Faces<BC> F;
+    const uint32_t gw = blockIdx.x * (uint32_t)(kPairThreads / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const uint32_t row = P.div_seg.div(gw);
+    if (row >= P.nrows) return;                       // whole warp
+    const int seg = (int)(gw - row * (uint32_t)P.nseg);
+    const uint32_t kk = P.div_m.div(row);
+    const int j = (int)(row - kk * (uint32_t)P.m) + 1;
+    const int k = (int)kk + 1;
+    const int i0 = seg * 64 + 2 * lane + 1;
+    const bool valid = i0 < P.l;                      // l even: the pair (i0, i0 + 1) is inside
+    const int ia = valid ? i0 : P.l - 1;              // other lanes read a valid pair, store nothing
+    const int nx = (int)P.nx, nxy = (int)P.nxy;
+    const int c = nx * j + nxy * k + ia;
+    if (OBS && P.obs != nullptr && j >= P.jmin - 1 && j <= P.jmax + 1 && k >= P.kmin - 1 && k <= P.kmax + 1 &&
+        seg * 64 + 64 >= P.imin - 1 && seg * 64 + 1 <= P.imax + 1) {
+        // the warp's 64 nodes touch the obstacle's box grown by one node:
+        // node by node with the one-node rules (each node reads and writes
+        // only slots no other node touches, so the order does not matter)
+        double m5[5];
+        if (valid) {
+            aa_odd_at<S, C, BC, int, CM, true, false>(P, ia, j, k, c, m5);
+            aa_odd_at<S, C, BC, int, CM, true, false>(P, ia + 1, j, k, c + 1, m5);
+        }
+        return;
+    }
+    if (BC != BC_DRIVEN || j == 1 || j == P.m || k == 1 || k == P.n)
+        aa_odd_pair_row<S, C, BC, CM, true>(P, j, k, lane, ia, valid, c);
+    else
+        aa_odd_pair_row<S, C, BC, CM, false>(P, j, k, lane, ia, valid, c);
 }
 
 // Outflow halo in slot form for a freshly loaded Layout E state: halo cell
