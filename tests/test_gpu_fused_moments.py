@@ -58,6 +58,25 @@ def test_lattice_step_moments(pattern, case):
     assert np.array_equal(a.download(), b.download())
 
 
+@pytest.mark.parametrize("pattern", ["ab", "aa"])
+def test_lattice_step_moments_many_groups(pattern):
+    """192 x 192 x 160 FP32 (thousands of blocks in the step with moments,
+    45 groups of the in-launch summation): the series against the separate
+    reduction after the same steps, and bit-identical on a second lattice
+    stepped the same way."""
+    from bgk3d_gpu_b200.lattice import Lattice
+    l, m, n = 192, 192, 160
+    st0 = random_state(l, m, n, 1, seed=21)
+    series = []
+    for _ in range(2):
+        lat = Lattice(l, m, n, kind=1, bcase="periodic", omega=OMEGA, pattern=pattern)
+        lat.upload(st0)
+        series.append(lat.step_moments(4, every=2))
+        close(series[-1][-1], lat.moments())
+        lat.close()
+    assert np.array_equal(series[0], series[1])
+
+
 def test_dropin_tracked_moments():
     import torch
     from bgk3d_gpu_b200 import _lib, load_dropin
